@@ -1,0 +1,499 @@
+#!/usr/bin/env python
+"""SpGEMM benchmark: C = A*A on the R-MAT 2^18 graph (average degree 16,
+(a,b,c,d) = (0.57,0.19,0.19,0.05), duplicates removed, values U(0,1]) on one
+B200 per process.
+
+One step = one complete product through the engine's C ABI: A given as CSC
+and B as CSR, already resident in HBM; symbolic pass, numeric pass and the
+sorted CSR of C (row pointers, columns, values) written to device memory.
+`value` = GFLOP/s counted as 2 x intermediate products, summed over ranks,
+with the time taken as the max over ranks of the summed per-step CUDA-event
+times (L2 flushed before every step: the inputs, 63 MB, fit in L2).
+
+Also printed on the same JSON line:
+  roofline      the dominant kernel's algorithmic bytes / its CUDA-event time,
+                against the measured HBM copy bandwidth;
+  pipeline      the same for the whole step;
+  e2e           the same metric through spgemm_multiply_host_to with pinned
+                host buffers: host->device copy of A and B, the product, and
+                the device->host copy of all of C inside the timed region;
+  cpu_baseline  the CPU restatement of the reference algorithm (FP32, all
+                host threads) on a bounded random sample of C's rows;
+  clocks        nvidia-smi samples taken during the timed region.
+
+--impl reference times that CPU restatement alone (the reference has no CPU
+multiply of its own and its GPU engine cannot run these inputs: int32
+overflow at P > 2^31, src/mm.cu:176-184).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpGEMM GFLOP/s + HBM GB/s vs roofline; batched/compensated vs plain at 1e-6"
+L2_FLUSH_BYTES = 512 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["rmat", "stencil", "stencil-comp", "er", "galerkin"],
+                   default="rmat")
+    p.add_argument("--scale", type=int, default=18, help="R-MAT scale (default 18)")
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=8.0)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+def build_workload(args):
+    from spgemm_b200 import workloads as W
+    if args.workload == "rmat":
+        A = W.rmat(args.scale, 16, 0)
+        return {"name": f"rmat{args.scale}_ef16_AxA", "products": [(A, A)], "precision": 0,
+                "config": {"workload": f"R-MAT 2^{args.scale} ef16 (0.57,0.19,0.19,0.05) dedup, "
+                                       "values U(0,1], C = A*A", "rows": A.rows, "nnz_a": A.nnz}}
+    if args.workload in ("stencil", "stencil-comp"):
+        A = W.stencil27(96, seed=0)
+        comp = args.workload == "stencil-comp"
+        return {"name": "stencil96_27pt_AxA" + ("_compensated" if comp else ""),
+                "products": [(A, A)], "precision": 1 if comp else 0,
+                "config": {"workload": "27-point stencil 96^3, random sign, |v| log-uniform "
+                                       f"[1e-4,1e4], C = A*A, {'compensated' if comp else 'plain'} FP32",
+                           "rows": A.rows, "nnz_a": A.nnz}}
+    if args.workload == "er":
+        A = W.er(4096, 8.0, 0)
+        return {"name": "er4096_AxA", "products": [(A, A)], "precision": 0,
+                "config": {"workload": "Erdos-Renyi 4096, 8/row, U[-1,1], C = A*A",
+                           "rows": A.rows, "nnz_a": A.nnz}}
+    if args.workload == "galerkin":
+        A = W.stencil27(64, values="laplace")
+        P = W.prolongator(64)
+        return {"name": "galerkin64_PtAP", "products": [(A, P), ("PT", "AP")], "precision": 1,
+                "A": A, "P": P,
+                "config": {"workload": "Galerkin P^T (A P), A 27-pt 64^3 (26/-1), P 2x2x2 "
+                                       "aggregates, compensated FP32", "rows": A.rows}}
+    raise ValueError(args.workload)
+
+
+def product_stats(A, B):
+    """Per-row P_i, nnz(A(i,:)) and the B bytes touched (for the roofline)."""
+    deg_b = np.diff(B.rowptr).astype(np.int64)
+    rows_of = np.repeat(np.arange(A.rows), np.diff(A.rowptr))
+    p_i = np.zeros(A.rows, np.int64)
+    np.add.at(p_i, rows_of, deg_b[A.col])
+    touched_k = np.zeros(B.rows, bool)
+    touched_k[A.col] = True
+    b_touched = 4 * (B.rows + 1) + 8 * int(deg_b[touched_k].sum())
+    return p_i, np.diff(A.rowptr).astype(np.int64), b_touched
+
+
+def sym_bin(p, n):
+    u = np.minimum(p, n)
+    lg = np.maximum(np.ceil(np.log2(np.maximum(2 * u, 1))).astype(np.int64), 6)
+    b = np.where((p <= 1024) & (lg <= 10), lg - 6, np.maximum(lg, 11) - 11 + 5)
+    b = np.where(p > 4096, 8, b)
+    return np.where(p <= 0, -1, b)
+
+
+def num_bin(o, p):
+    lg = np.maximum(np.ceil(np.log2(np.maximum(2 * o, 1))).astype(np.int64), 6)
+    b = np.where((p <= 2048) & (lg <= 9), lg - 6, np.maximum(lg, 10) - 10 + 4)
+    b = np.where(o > 4096, 8, b)
+    return np.where(o <= 0, -1, b)
+
+
+def kernel_bin(name):
+    """(pass, bin) of an engine kernel name, or None."""
+    import re
+    m = re.match(r"k_(sym|num)_(warp|block)<(\d+)>", name)
+    if m:
+        lg = int(m.group(3))
+        if m.group(1) == "sym":
+            return ("sym", lg - 6 if m.group(2) == "warp" else lg - 11 + 5)
+        return ("num", lg - 6 if m.group(2) == "warp" else lg - 10 + 4)
+    if name.startswith("k_sym_long"):
+        return ("sym", 8)
+    if name.startswith("k_num_long"):
+        return ("num", 8)
+    return None
+
+
+def algorithmic_bytes(rows_sel, p_i, a_len, o_i, b_touched, p_total, with_c=True):
+    """The bytes of A + B rows touched + 8 bytes per partial + C (the
+    roofline's algorithmic bytes) restricted to the selected rows; B's share
+    is apportioned by partial products."""
+    p = int(p_i[rows_sel].sum())
+    a = 4 * (int(rows_sel.sum()) + 1) + 8 * int(a_len[rows_sel].sum())
+    b = int(round(b_touched * (p / max(p_total, 1))))
+    c = (4 * (int(rows_sel.sum()) + 1) + 8 * int(o_i[rows_sel].sum())) if with_c else 4 * int(rows_sel.sum())
+    return a + b + 8 * p + c
+
+
+# ---------------------------------------------------------------------------
+# measurement helpers
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"spgemm_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"], f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(A, B, target_seconds, seed=0):
+    """FP32 CPU restatement of the reference algorithm (oracle mode 1), all
+    host threads, on a random sample of rows sized for ~target_seconds."""
+    import oracle
+    a = A.to_csc()
+    threads = os.cpu_count() or 1
+    p_i, _, _ = product_stats(A, B)
+    rng = np.random.default_rng(seed)
+    order = rng.permutation(A.rows).astype(np.int32)
+    csum = np.cumsum(p_i[order])
+
+    def run(target_p):
+        k = int(np.searchsorted(csum, target_p)) + 1
+        rows = np.sort(order[:min(k, A.rows)])
+        t0 = time.perf_counter()
+        r = oracle.spgemm(A.rows, B.cols, a.colptr, a.rowidx, a.val, B.rowptr, B.col, B.val,
+                          rows=rows, mode=1, threads=threads)
+        dt = time.perf_counter() - t0
+        return dt, r["products"], len(rows)
+
+    dt, prods, _ = run(min(2e7, csum[-1]))
+    rate = prods / max(dt, 1e-9)
+    target = min(rate * target_seconds, float(csum[-1]))
+    dt, prods, nrows = run(target)
+    return {"value": 2.0 * prods / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+            "sample": f"{nrows} random rows of C ({prods} of {int(csum[-1])} products, "
+                      f"{100.0 * prods / csum[-1]:.1f}%), {dt:.2f} s"}, (dt, prods, nrows)
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = build_workload(args)
+    A, B = wl["products"][0]
+    if isinstance(A, str):
+        A, B = wl["A"], wl["P"]
+    for _ in range(args.warmup):
+        cpu_baseline(A, B, 1.0)
+    vals = []
+    last = None
+    for k in range(args.steps):
+        cb, last = cpu_baseline(A, B, 4.0, seed=k)
+        vals.append(cb["value"])
+    value = float(np.mean(vals))
+    dt, prods, nrows = last
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "GFLOP/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": wl["config"],
+            "cpu_baseline": {"value": value, "unit": "GFLOP/s", "cores": os.cpu_count(),
+                             "kind": "port",
+                             "sample": f"per step: random rows of C sized for ~4 s "
+                                       f"(last: {nrows} rows, {prods} products)"},
+            "e2e": {"value": value, "unit": "GFLOP/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "the reference has no CPU multiply; this is the oracle's FP32 restatement "
+                    "of its algorithm (src/mm.cu initGEMM/binGEMM/mergeGEMM), all host threads"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import spgemm_b200 as sg
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    wl = build_workload(args)
+    stream = torch.cuda.current_stream()
+
+    def to_dev(a, dt):
+        return torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype=dt)
+
+    handles, steps_fn, keep = [], None, []
+    if args.workload == "galerkin":
+        A, P = wl["A"], wl["P"]
+        Ac = A.to_csc()
+        tA = [to_dev(Ac.colptr, torch.int32), to_dev(Ac.rowidx, torch.int32), to_dev(Ac.val, torch.float32)]
+        tP = [to_dev(P.rowptr, torch.int32), to_dev(P.col, torch.int32), to_dev(P.val, torch.float32)]
+        keep += tA + tP
+        A_cm = sg.device_cm(tA[0].data_ptr(), tA[1].data_ptr(), tA[2].data_ptr(), A.nnz, A.rows, A.cols, sg.COL_MAJOR)
+        P_cm = sg.device_cm(tP[0].data_ptr(), tP[1].data_ptr(), tP[2].data_ptr(), P.nnz, P.rows, P.cols, sg.ROW_MAJOR)
+        PT_cm = sg.device_cm(tP[0].data_ptr(), tP[1].data_ptr(), tP[2].data_ptr(), P.nnz, P.cols, P.rows, sg.COL_MAJOR)
+        h1, h2 = sg.Handle(wl["precision"]), sg.Handle(wl["precision"])
+        handles = [h1, h2]
+
+        def step():
+            AP = h1.multiply(A_cm, P_cm)
+            h2.multiply(PT_cm, AP)
+        ap_nnz = 0
+        p1 = product_stats(A, P)[0].sum()
+        flops_per_step = None
+    else:
+        A, B = wl["products"][0]
+        Ac = A.to_csc()
+        tA = [to_dev(Ac.colptr, torch.int32), to_dev(Ac.rowidx, torch.int32), to_dev(Ac.val, torch.float32)]
+        tB = [to_dev(B.rowptr, torch.int32), to_dev(B.col, torch.int32), to_dev(B.val, torch.float32)]
+        keep += tA + tB
+        A_cm = sg.device_cm(tA[0].data_ptr(), tA[1].data_ptr(), tA[2].data_ptr(), A.nnz, A.rows, A.cols, sg.COL_MAJOR)
+        B_cm = sg.device_cm(tB[0].data_ptr(), tB[1].data_ptr(), tB[2].data_ptr(), B.nnz, B.rows, B.cols, sg.ROW_MAJOR)
+        h1 = sg.Handle(wl["precision"])
+        handles = [h1]
+        out = {}
+
+        def step():
+            nnz = h1.symbolic(A_cm, B_cm)
+            if out.get("cap", -1) < nnz:  # first call only: same product every step
+                out["rowptr"] = torch.empty(A.rows + 1, dtype=torch.int32, device=dev)
+                out["col"] = torch.empty(max(nnz, 1), dtype=torch.int32, device=dev)
+                out["val"] = torch.empty(max(nnz, 1), dtype=torch.float32, device=dev)
+                out["cap"] = nnz
+            h1.numeric(out["rowptr"].data_ptr(), out["col"].data_ptr(), out["val"].data_ptr())
+    for h in handles:
+        h.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    stats = [h.stats() for h in handles]
+    products = sum(s["intermediate_products"] for s in stats)
+    nnz_c = stats[-1]["nnz_c"]
+    launches0 = sum(s["kernel_launches"] for s in stats)
+    for h in handles:
+        h.reset_kernel_times()
+        h.set_profiling(True)
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    smi_id = vis.split(",")[local].strip() if vis else str(local)
+    sampler = ClockSampler(smi_id) if rank == 0 else None
+    if sampler:
+        sampler.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()
+        ev[k][0].record(stream)
+        step()
+        ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    launches = sum(h.stats()["kernel_launches"] for h in handles) - launches0
+    ktimes = {}
+    for h in handles:
+        h.set_profiling(False)
+        for name, (ms, cnt) in h.kernel_times().items():
+            t = ktimes.get(name, (0.0, 0))
+            ktimes[name] = (t[0] + ms, t[1] + cnt)
+    if dist:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    flops = 2.0 * products * args.steps * world
+    value = flops / (total_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+
+    # roofline of the dominant kernel + the whole pipeline
+    roof, pipeline = None, None
+    if args.workload != "galerkin" and rank == 0:
+        A, B = wl["products"][0]
+        p_i, a_len, b_touched = product_stats(A, B)
+        crow = out["rowptr"].cpu().numpy()
+        o_i = np.diff(crow.astype(np.int64))
+        total_alg = algorithmic_bytes(np.ones(A.rows, bool), p_i, a_len, o_i, b_touched, products)
+        pipeline = {"algorithmic_bytes": total_alg, "gbs": total_alg / (total_ms / args.steps / 1e3) / 1e9 / world,
+                    "frac": total_alg / (total_ms / args.steps / 1e3) / 1e9 / world / peak}
+        dom = max(ktimes.items(), key=lambda kv: kv[1][0]) if ktimes else None
+        if dom:
+            name, (ms, cnt) = dom
+            kb = kernel_bin(name)
+            if kb:
+                pas, b = kb
+                sel = (sym_bin(p_i, B.cols) == b) if pas == "sym" else (num_bin(o_i, p_i) == b)
+                alg = algorithmic_bytes(sel, p_i, a_len, o_i, b_touched, products,
+                                        with_c=(pas == "num"))
+                per_launch = alg * args.steps / cnt
+                avg_s = ms / cnt / 1e3
+                roof = {"bound": "hbm", "kernel": name, "achieved": per_launch / avg_s / 1e9,
+                        "peak": peak, "unit": "GB/s", "frac": per_launch / avg_s / 1e9 / peak,
+                        "traffic": None, "algorithmic_bytes_per_launch": per_launch,
+                        "avg_launch_ms": ms / cnt, "peak_kind": peak_kind}
+        pipeline["kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][0])}
+
+    # e2e through the host-buffer C ABI (pinned host memory)
+    e2e = None
+    if not args.no_e2e and args.workload != "galerkin":
+        A, B = wl["products"][0]
+        Ac = A.to_csc()
+        pin = lambda a, dt: torch.from_numpy(np.ascontiguousarray(a)).to(dt).pin_memory()
+        hA = [pin(Ac.colptr, torch.int32), pin(Ac.rowidx, torch.int32), pin(Ac.val, torch.float32)]
+        hB = [pin(B.rowptr, torch.int32), pin(B.col, torch.int32), pin(B.val, torch.float32)]
+        try:
+            o_rp = torch.empty(A.rows + 1, dtype=torch.int32).pin_memory()
+            o_col = torch.empty(nnz_c, dtype=torch.int32).pin_memory()
+            o_val = torch.empty(nnz_c, dtype=torch.float32).pin_memory()
+            pinned_out = True
+        except RuntimeError:
+            o_rp = torch.empty(A.rows + 1, dtype=torch.int32)
+            o_col = torch.empty(nnz_c, dtype=torch.int32)
+            o_val = torch.empty(nnz_c, dtype=torch.float32)
+            pinned_out = False
+        Ah = sg.Csc(A.rows, A.cols, hA[0].numpy(), hA[1].numpy(), hA[2].numpy())
+        Bh = sg.Csr(B.rows, B.cols, hB[0].numpy(), hB[1].numpy(), hB[2].numpy())
+        he = sg.Handle(wl["precision"])
+        he.set_stream(stream.cuda_stream)
+        h2d = sum(t.numel() * 4 for t in hA + hB)
+        d2h = (A.rows + 1 + 2 * nnz_c) * 4
+        he.multiply_host_to(Ah, Bh, o_rp.numpy(), o_col.numpy(), o_val.numpy())  # warm-up
+        torch.cuda.synchronize()
+        e_ms = []
+        for _ in range(args.e2e_steps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            flush.zero_()
+            s.record(stream)
+            he.multiply_host_to(Ah, Bh, o_rp.numpy(), o_col.numpy(), o_val.numpy())
+            e.record(stream)
+            torch.cuda.synchronize()
+            e_ms.append(s.elapsed_time(e))
+        he.close()
+        e_total = float(sum(e_ms))
+        if dist:
+            t = torch.tensor([e_total], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_total = float(t.item())
+        e2e = {"value": 2.0 * products * len(e_ms) * world / (e_total / 1e3) / 1e9, "unit": "GFLOP/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": e_total / len(e_ms), "pinned_output": pinned_out}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        A, B = (wl["A"], wl["P"]) if args.workload == "galerkin" else wl["products"][0]
+        cpu, _ = cpu_baseline(A, B, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded generator; the reference's SuiteSparse/SNAP inputs are not available)",
+                "config": dict(wl["config"], intermediate_products=products, nnz_c=nnz_c,
+                               l2="flushed before every step (512 MiB write)",
+                               parallelism=f"replicas x{world} (one independent product per GPU)"),
+                "roofline": roof, "pipeline": pipeline, "cpu_baseline": cpu, "e2e": e2e,
+                "clocks": clocks, "gpu_launches": launches,
+                "step_ms": step_ms}
+        print(json.dumps(line), flush=True)
+    for h in handles:
+        h.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,138 @@
+/* spgemm_b200: handle-based C ABI of the sm_100a SpGEMM engine.
+ *
+ * Computes C = A * B for sparse FP32 matrices. A is given as CSC (type
+ * COL_MAJOR, the layout the reference engine consumes, reference
+ * src/mm.cu:87-109) or CSR (type ROW_MAJOR); B is CSR. C is produced as CSR
+ * with column indices sorted ascending inside every row. The structure of C
+ * is the symbolic union of the partial products: an entry exists wherever at
+ * least one product A(i,k)*B(k,j) is formed, even when the products cancel
+ * to exactly zero (the reference keeps such entries too: it emits a column
+ * on first touch, src/mm.cu:386-391, and counts it in nnzC, src/mm.cu:432).
+ *
+ * Matrices are passed as the reference's `cm` struct (cm.h) holding DEVICE
+ * pointers unless a function says otherwise. Every call is asynchronous on
+ * the handle's stream except where it must return a count to the host
+ * (spgemm_symbolic, spgemm_multiply), which synchronises that stream.
+ *
+ * Errors: every function returns an spgemm_status; the last failure's text
+ * is kept per handle (spgemm_last_error). Nothing calls exit().
+ * The reference has no handle API; its error path prints and exits
+ * (src/mm.cu:6-14). The legacy shims in mm.h keep that behaviour.
+ */
+#ifndef SPGEMM_B200_H_
+#define SPGEMM_B200_H_
+
+#include <stddef.h>
+#include "cm.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum spgemm_status {
+    SPGEMM_OK = 0,
+    SPGEMM_ERR_INVALID = 1,     /* bad argument: shape, type, null pointer */
+    SPGEMM_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    SPGEMM_ERR_ALLOC = 3,       /* device or host allocation failed */
+    SPGEMM_ERR_OVERFLOW = 4,    /* nnz(C) does not fit the int32 CSR of cm */
+    SPGEMM_ERR_STATE = 5,       /* call out of order (e.g. numeric before symbolic) */
+    SPGEMM_ERR_DEVICE = 6,      /* a kernel's own range check tripped */
+    SPGEMM_ERR_TOO_LARGE = 7    /* a size exceeds a documented maximum */
+} spgemm_status;
+
+typedef enum spgemm_precision {
+    /* FP32 products, FP32 accumulation. */
+    SPGEMM_PRECISION_PLAIN = 0,
+    /* FP32 products with their FMA rounding error (TwoProduct) and
+     * TwoSum-compensated FP32 accumulation (Ogita, Rump & Oishi, "Accurate
+     * Sum and Dot Product", SIAM J. Sci. Comput. 26(6), 2005, Dot2); rows
+     * with more than 4096 partial products accumulate in FP64 instead. */
+    SPGEMM_PRECISION_COMPENSATED = 1
+} spgemm_precision;
+
+typedef struct spgemm_context* spgemm_handle_t;
+
+/* Per-product statistics of the last symbolic/multiply call. */
+typedef struct spgemm_stats {
+    long long intermediate_products;   /* P = sum_k nnz(A(:,k)) * nnz(B(k,:)) */
+    long long nnz_c;                   /* exact nnz(C) */
+    int rows_per_symbolic_bin[16];     /* rows handled by each symbolic bin */
+    int rows_per_numeric_bin[16];      /* rows handled by each numeric bin */
+    int long_row_slices;               /* column slices of the long-row path */
+    long long kernel_launches;         /* engine kernels launched by the handle so far */
+} spgemm_stats;
+
+/* Library version string. */
+const char* spgemm_version(void);
+/* Human-readable text of a status code. */
+const char* spgemm_status_string(int status);
+
+/* Create a handle bound to the current CUDA device; its stream is the
+ * default stream until spgemm_set_stream. */
+int spgemm_create(spgemm_handle_t* handle);
+/* Free the handle and every device buffer it owns. */
+int spgemm_destroy(spgemm_handle_t handle);
+/* Use `stream` (a cudaStream_t) for all later work of the handle. */
+int spgemm_set_stream(spgemm_handle_t handle, void* stream);
+/* Select SPGEMM_PRECISION_PLAIN or SPGEMM_PRECISION_COMPENSATED. */
+int spgemm_set_precision(spgemm_handle_t handle, int precision);
+/* Text of the handle's last error ("" if none). */
+const char* spgemm_last_error(spgemm_handle_t handle);
+
+/* Phase 1: row analysis, binning and the symbolic pass of C = A*B.
+ * Writes the exact nnz(C) to *nnz_c. A: CSC (COL_MAJOR) or CSR (ROW_MAJOR);
+ * B: CSR. A.num_cols must equal B.num_rows. Device pointers; the arrays must
+ * stay valid and unchanged until spgemm_numeric returns. */
+int spgemm_symbolic(spgemm_handle_t handle, cm A, cm B, long long* nnz_c);
+/* Phase 2: numeric pass into caller-allocated device buffers:
+ * c_rowptr[A rows + 1], c_colidx[nnz_c], c_val[nnz_c]. */
+int spgemm_numeric(spgemm_handle_t handle, int* c_rowptr, int* c_colidx,
+                   float* c_val);
+/* Both phases into handle-owned device buffers (valid until the next call
+ * on the handle or spgemm_destroy); *C receives device pointers and sizes. */
+int spgemm_multiply(spgemm_handle_t handle, cm A, cm B, cm* C);
+/* Statistics of the last product. */
+int spgemm_get_stats(spgemm_handle_t handle, spgemm_stats* out);
+
+/* Host-buffer convenience: copies A (CSC or CSR) and B (CSR) from host
+ * memory, multiplies, and returns C as host CSR with malloc'd arrays
+ * (release with cmFree). */
+int spgemm_multiply_host(spgemm_handle_t handle, cm A_host, cm B_host,
+                         cm* C_host);
+/* Host-buffer variant writing into caller-provided host arrays (which may
+ * be pinned): c_rowptr[A rows + 1], c_colidx/c_val[capacity]. *nnz_c
+ * receives nnz(C); SPGEMM_ERR_TOO_LARGE when it exceeds `capacity` (nothing
+ * is written then, and the call can be repeated with larger arrays). */
+int spgemm_multiply_host_to(spgemm_handle_t handle, cm A_host, cm B_host,
+                            int* c_rowptr, int* c_colidx, float* c_val,
+                            long long capacity, long long* nnz_c);
+
+/* Per-kernel timing: when enabled, CUDA events are recorded on the handle's
+ * stream around every engine kernel launch and accumulated per kernel name
+ * (collected at the end of each numeric pass). */
+int spgemm_set_profiling(spgemm_handle_t handle, int enable);
+int spgemm_reset_kernel_times(spgemm_handle_t handle);
+/* Writes up to max_kernels entries: names ('\n'-separated into `names`),
+ * accumulated milliseconds and launch counts. Returns the entry count (or a
+ * negated status). */
+int spgemm_get_kernel_times(spgemm_handle_t handle, char* names, int names_len,
+                            double* ms, long long* launches, int max_kernels);
+
+/* Companion of the mm.h shims: copy the C that cudaMergeGEMM produced into
+ * malloc'd host arrays (sorted CSR, nnz = exact nnz(C)). Returns 0 on
+ * success. The reference never returns C (src/mm.cu:420-449). */
+int spgemm_get_result(cm* C_host_out);
+/* mm.h shims print like the reference (P at cudaInitGEMM, "nnzC nnzCf" at
+ * cudaMergeGEMM) when verbose is 1 (default); 0 silences them. */
+void spgemm_set_verbose(int verbose);
+/* mm.h shims call exit(-1) on a CUDA error like the reference when 1
+ * (default); 0 makes them print and return instead. */
+void spgemm_set_exit_on_error(int enable);
+/* Status of the last mm.h shim call (SPGEMM_OK if it succeeded). */
+int spgemm_legacy_status(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPGEMM_B200_H_ */

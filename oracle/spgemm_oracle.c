@@ -1,0 +1,354 @@
+/* CPU oracle for the SpGEMM path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load this library, and only as the checker / the timed CPU baseline. The
+ * product path (spgemm_b200) never calls it.
+ *
+ * It restates the algorithm of the reference's live engine, src/mm.cu:
+ *   1. symbolic upper bound per C row (initGEMM, src/mm.cu:138-148):
+ *        row_p[i] = sum over A(i,k) != 0 of nnz(B(k,:));
+ *   2. outer-product expansion into row buckets (binGEMM, src/mm.cu:288-312):
+ *        for k ascending, for every A(i,k): append A(i,k) * B(k,j) for each
+ *        j in B(k,:) (column order) to bucket i;
+ *   3. per-row merge with a dense accumulator (mergeGEMM, src/mm.cu:366-404).
+ * with the reference's defects fixed as follows (they are documented in the
+ * reference's source and make its own output unusable as a check):
+ *   - the merge accumulates in floating point (the reference's dense array
+ *     is int*, src/mm.cu:33,386, truncating every partial);
+ *   - a column is emitted on its FIRST touch, tracked by a flag (the
+ *     reference tests |old| < 1e-4, src/mm.cu:387, which re-emits a column
+ *     after cancellation and drops none);
+ *   - emitted columns are sorted ascending (the reference's order is atomic
+ *     arrival order, src/mm.cu:389-390);
+ *   - every k is expanded (the reference drops columns k with
+ *     nnz(B(k,:)) >= 128 that are not in the heavy bin, src/mm.cu:213-221);
+ *   - counts and offsets are 64-bit (the reference overflows int at
+ *     P > 2^31, src/mm.cu:176-184).
+ * Explicit zeros are kept: an entry exists wherever a product lands, as in
+ * the reference (emitted on first touch regardless of value, counted in
+ * nnzC at src/mm.cu:432).
+ *
+ * Bucket i holds its products in k-ascending order, which is exactly the
+ * order in which row i of the k-ascending CSR transpose of A visits B's
+ * rows; the oracle therefore builds that transpose once and fills each
+ * bucket row by row, so memory stays bounded by one bucket per thread.
+ *
+ * Precision: mode 0 forms products and sums in double (the FP64 oracle:
+ * products of two floats are exact in double); mode 1 forms and sums them
+ * in float (the FP32 CPU baseline, reported only). Mode 0 can also return,
+ * per entry, the sum of |product| and the number of products, from which
+ * the tests derive summation-error bounds.
+ *
+ * Parity pinning: the reference has no CPU multiply and no tests or golden
+ * vectors (its merge is defective as listed above and its GPU code reads and
+ * writes out of bounds, src/mm.cu:200,374-402), so this restatement is
+ * pinned to the reference only through its host reader/sort (compiled from
+ * the reference sources into oracle/_ref and compared in the tests) and
+ * the intermediate-product count P it prints (src/mm.cu:181). The multiply
+ * itself is cross-checked against scipy.sparse and hand-computed products.
+ * Parity of the multiply is therefore unpinned by the reference itself.
+ */
+#include <math.h>
+#include <pthread.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct oracle_csr {
+  int nrows;          /* number of computed rows */
+  long long nnz;
+  long long products; /* P over the computed rows */
+  long long* rowptr;  /* nrows + 1 */
+  int* col;           /* nnz */
+  double* val;        /* mode 0: nnz values */
+  float* val32;       /* mode 1: nnz values */
+  double* absum;      /* mode 0 with stats: sum of |product| per entry */
+  int* nterms;        /* mode 0 with stats: products per entry */
+} oracle_csr;
+
+/* Step 1 alone (initGEMM): per-row product counts from A in CSC.
+ * Returns P. row_p may be NULL. */
+long long oracle_count_products(int m, int kdim, const int* a_colptr, const int* a_rowidx,
+                                const int* b_rowptr, long long* row_p) {
+  long long total = 0;
+  if (row_p) memset(row_p, 0, sizeof(long long) * (size_t)m);
+  for (int k = 0; k < kdim; ++k) {
+    const long long len = b_rowptr[k + 1] - b_rowptr[k];
+    for (int e = a_colptr[k]; e < a_colptr[k + 1]; ++e) {
+      const int i = a_rowidx[e];
+      if (i < 0 || i >= m) continue;
+      if (row_p) row_p[i] += len;
+      total += len;
+    }
+  }
+  return total;
+}
+
+typedef struct {
+  /* shared inputs */
+  int m, n;
+  const int* at_ptr;  /* k-ascending CSR transpose of A */
+  const int* at_k;
+  const float* at_v;
+  const int* b_rowptr;
+  const int* b_colidx;
+  const float* b_val;
+  const int* rows;
+  int mode, want_stats;
+  /* this thread's rows: rows[r0 .. r1) */
+  int r0, r1;
+  /* outputs */
+  long long nnz, products;
+  long long* counts; /* r1 - r0 */
+  int* col;
+  double* val;
+  float* val32;
+  double* absum;
+  int* nterms;
+  long long cap;
+  int failed;
+} worker_t;
+
+static int grow(worker_t* w, long long need) {
+  if (need <= w->cap) return 1;
+  long long nc = w->cap ? w->cap : 1024;
+  while (nc < need) nc *= 2;
+  int* c = (int*)realloc(w->col, sizeof(int) * (size_t)nc);
+  if (!c) return 0;
+  w->col = c;
+  if (w->mode == 0) {
+    double* v = (double*)realloc(w->val, sizeof(double) * (size_t)nc);
+    if (!v) return 0;
+    w->val = v;
+    if (w->want_stats) {
+      double* a = (double*)realloc(w->absum, sizeof(double) * (size_t)nc);
+      int* t = (int*)realloc(w->nterms, sizeof(int) * (size_t)nc);
+      if (a) w->absum = a;
+      if (t) w->nterms = t;
+      if (!a || !t) return 0;
+    }
+  } else {
+    float* v = (float*)realloc(w->val32, sizeof(float) * (size_t)nc);
+    if (!v) return 0;
+    w->val32 = v;
+  }
+  w->cap = nc;
+  return 1;
+}
+
+static int cmp_int(const void* a, const void* b) {
+  const int x = *(const int*)a, y = *(const int*)b;
+  return (x > y) - (x < y);
+}
+
+static void* worker_run(void* arg) {
+  worker_t* w = (worker_t*)arg;
+  const int n = w->n;
+  /* dense accumulator + first-touch flags (mergeGEMM's dense row) */
+  double* acc = (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  float* acc32 = (float*)calloc((size_t)(n > 0 ? n : 1), sizeof(float));
+  double* aabs = w->want_stats ? (double*)calloc((size_t)(n > 0 ? n : 1), sizeof(double)) : NULL;
+  int* aterm = w->want_stats ? (int*)calloc((size_t)(n > 0 ? n : 1), sizeof(int)) : NULL;
+  unsigned char* touched = (unsigned char*)calloc((size_t)(n > 0 ? n : 1), 1);
+  int* emitted = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+  /* bucket of one row: (column, product) in expansion order */
+  long long bcap = 1 << 16;
+  int* bcol = (int*)malloc(sizeof(int) * (size_t)bcap);
+  double* bval = (double*)malloc(sizeof(double) * (size_t)bcap);
+  float* bval32 = (float*)malloc(sizeof(float) * (size_t)bcap);
+  w->counts = (long long*)calloc((size_t)(w->r1 - w->r0 + 1), sizeof(long long));
+  if (!acc || !acc32 || !touched || !emitted || !bcol || !bval || !bval32 || !w->counts ||
+      (w->want_stats && (!aabs || !aterm))) {
+    w->failed = 1;
+    goto done;
+  }
+  for (int r = w->r0; r < w->r1; ++r) {
+    const int i = w->rows ? w->rows[r] : r;
+    /* step 2: fill bucket i, k ascending */
+    long long nb = 0;
+    for (int e = w->at_ptr[i]; e < w->at_ptr[i + 1]; ++e) {
+      const int k = w->at_k[e];
+      const float a = w->at_v[e];
+      const int bs = w->b_rowptr[k], be = w->b_rowptr[k + 1];
+      if (nb + (be - bs) > bcap) {
+        while (nb + (be - bs) > bcap) bcap *= 2;
+        int* c2 = (int*)realloc(bcol, sizeof(int) * (size_t)bcap);
+        double* v2 = (double*)realloc(bval, sizeof(double) * (size_t)bcap);
+        float* v3 = (float*)realloc(bval32, sizeof(float) * (size_t)bcap);
+        if (c2) bcol = c2;
+        if (v2) bval = v2;
+        if (v3) bval32 = v3;
+        if (!c2 || !v2 || !v3) { w->failed = 1; goto done; }
+      }
+      for (int q = bs; q < be; ++q) {
+        bcol[nb] = w->b_colidx[q];
+        if (w->mode == 0) bval[nb] = (double)a * (double)w->b_val[q];
+        else bval32[nb] = a * w->b_val[q];
+        ++nb;
+      }
+    }
+    w->products += nb;
+    /* step 3: merge with first-touch flags */
+    int ne = 0;
+    for (long long q = 0; q < nb; ++q) {
+      const int c = bcol[q];
+      if (c < 0 || c >= n) continue;
+      if (!touched[c]) { touched[c] = 1; emitted[ne++] = c; }
+      if (w->mode == 0) {
+        acc[c] += bval[q];
+        if (aabs) { aabs[c] += fabs(bval[q]); aterm[c] += 1; }
+      } else {
+        acc32[c] += bval32[q];
+      }
+    }
+    qsort(emitted, (size_t)ne, sizeof(int), cmp_int);
+    if (!grow(w, w->nnz + ne)) { w->failed = 1; goto done; }
+    for (int t = 0; t < ne; ++t) {
+      const int c = emitted[t];
+      const long long o = w->nnz + t;
+      w->col[o] = c;
+      if (w->mode == 0) {
+        w->val[o] = acc[c];
+        acc[c] = 0.0;
+        if (aabs) { w->absum[o] = aabs[c]; w->nterms[o] = aterm[c]; aabs[c] = 0.0; aterm[c] = 0; }
+      } else {
+        w->val32[o] = acc32[c];
+        acc32[c] = 0.f;
+      }
+      touched[c] = 0;
+    }
+    w->counts[r - w->r0] = ne;
+    w->nnz += ne;
+  }
+done:
+  free(acc); free(acc32); free(aabs); free(aterm); free(touched); free(emitted);
+  free(bcol); free(bval); free(bval32);
+  return NULL;
+}
+
+void oracle_free(oracle_csr* r) {
+  if (!r) return;
+  free(r->rowptr); free(r->col); free(r->val); free(r->val32); free(r->absum); free(r->nterms);
+  free(r);
+}
+
+/* C = A * B for the listed rows of C (rows == NULL: all m rows, in order).
+ * A: CSC (a_colptr[kdim+1], a_rowidx, a_val); B: CSR (b_rowptr[kdim+1],
+ * b_colidx, b_val); C has n columns. Rows are split over `nthreads`
+ * pthreads by product count. Returns NULL on allocation failure. */
+oracle_csr* oracle_spgemm(int m, int kdim, int n, const int* a_colptr, const int* a_rowidx,
+                          const float* a_val, const int* b_rowptr, const int* b_colidx,
+                          const float* b_val, const int* rows, int nrows, int mode,
+                          int want_stats, int nthreads) {
+  if (!rows) nrows = m;
+  if (nthreads < 1) nthreads = 1;
+  oracle_csr* res = (oracle_csr*)calloc(1, sizeof(oracle_csr));
+  if (!res) return NULL;
+  const int nnz_a = a_colptr[kdim];
+  /* k-ascending transpose of A (stable counting sort of CSC by row) */
+  int* at_ptr = (int*)calloc((size_t)m + 1, sizeof(int));
+  int* at_k = (int*)malloc(sizeof(int) * (size_t)(nnz_a > 0 ? nnz_a : 1));
+  float* at_v = (float*)malloc(sizeof(float) * (size_t)(nnz_a > 0 ? nnz_a : 1));
+  int* cur = (int*)malloc(sizeof(int) * (size_t)(m > 0 ? m : 1));
+  long long* row_p = (long long*)calloc((size_t)(m > 0 ? m : 1), sizeof(long long));
+  worker_t* ws = (worker_t*)calloc((size_t)nthreads, sizeof(worker_t));
+  pthread_t* th = (pthread_t*)calloc((size_t)nthreads, sizeof(pthread_t));
+  if (!at_ptr || !at_k || !at_v || !cur || !row_p || !ws || !th) goto fail;
+  for (int e = 0; e < nnz_a; ++e) {
+    const int i = a_rowidx[e];
+    if (i >= 0 && i < m) at_ptr[i + 1]++;
+  }
+  for (int i = 0; i < m; ++i) at_ptr[i + 1] += at_ptr[i];
+  memcpy(cur, at_ptr, sizeof(int) * (size_t)(m > 0 ? m : 1));
+  for (int k = 0; k < kdim; ++k)
+    for (int e = a_colptr[k]; e < a_colptr[k + 1]; ++e) {
+      const int i = a_rowidx[e];
+      if (i < 0 || i >= m) continue;
+      const int p = cur[i]++;
+      at_k[p] = k;
+      at_v[p] = a_val[e];
+    }
+  oracle_count_products(m, kdim, a_colptr, a_rowidx, b_rowptr, row_p);
+  /* split rows[0..nrows) into nthreads contiguous groups of similar work */
+  {
+    long long total = 0;
+    for (int r = 0; r < nrows; ++r) total += row_p[rows ? rows[r] : r] + 1;
+    long long run = 0;
+    int t = 0, start = 0;
+    for (int r = 0; r < nrows && t < nthreads - 1; ++r) {
+      run += row_p[rows ? rows[r] : r] + 1;
+      if (run * nthreads >= total * (t + 1)) {
+        ws[t].r0 = start;
+        ws[t].r1 = r + 1;
+        start = r + 1;
+        ++t;
+      }
+    }
+    for (; t < nthreads; ++t) { ws[t].r0 = start; ws[t].r1 = nrows; start = nrows; }
+  }
+  for (int t = 0; t < nthreads; ++t) {
+    worker_t* w = &ws[t];
+    w->m = m; w->n = n;
+    w->at_ptr = at_ptr; w->at_k = at_k; w->at_v = at_v;
+    w->b_rowptr = b_rowptr; w->b_colidx = b_colidx; w->b_val = b_val;
+    w->rows = rows; w->mode = mode; w->want_stats = mode == 0 && want_stats;
+  }
+  if (nthreads == 1) {
+    worker_run(&ws[0]);
+  } else {
+    for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, worker_run, &ws[t]);
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+  }
+  for (int t = 0; t < nthreads; ++t)
+    if (ws[t].failed) goto fail;
+  /* concatenate in row order */
+  {
+    long long nnz = 0, prod = 0;
+    for (int t = 0; t < nthreads; ++t) { nnz += ws[t].nnz; prod += ws[t].products; }
+    res->nrows = nrows;
+    res->nnz = nnz;
+    res->products = prod;
+    res->rowptr = (long long*)malloc(sizeof(long long) * ((size_t)nrows + 1));
+    res->col = (int*)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    if (mode == 0) res->val = (double*)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+    else res->val32 = (float*)malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1));
+    if (mode == 0 && want_stats) {
+      res->absum = (double*)malloc(sizeof(double) * (size_t)(nnz > 0 ? nnz : 1));
+      res->nterms = (int*)malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1));
+    }
+    if (!res->rowptr || !res->col || (mode == 0 && !res->val) || (mode == 1 && !res->val32) ||
+        (mode == 0 && want_stats && (!res->absum || !res->nterms)))
+      goto fail;
+    long long o = 0;
+    res->rowptr[0] = 0;
+    for (int t = 0; t < nthreads; ++t) {
+      worker_t* w = &ws[t];
+      for (int r = w->r0; r < w->r1; ++r) res->rowptr[r + 1] = res->rowptr[r] + w->counts[r - w->r0];
+      if (w->nnz) {
+        memcpy(res->col + o, w->col, sizeof(int) * (size_t)w->nnz);
+        if (mode == 0) memcpy(res->val + o, w->val, sizeof(double) * (size_t)w->nnz);
+        else memcpy(res->val32 + o, w->val32, sizeof(float) * (size_t)w->nnz);
+        if (mode == 0 && want_stats) {
+          memcpy(res->absum + o, w->absum, sizeof(double) * (size_t)w->nnz);
+          memcpy(res->nterms + o, w->nterms, sizeof(int) * (size_t)w->nnz);
+        }
+      }
+      o += w->nnz;
+    }
+  }
+  for (int t = 0; t < nthreads; ++t) {
+    free(ws[t].counts); free(ws[t].col); free(ws[t].val); free(ws[t].val32);
+    free(ws[t].absum); free(ws[t].nterms);
+  }
+  free(at_ptr); free(at_k); free(at_v); free(cur); free(row_p); free(ws); free(th);
+  return res;
+fail:
+  if (ws)
+    for (int t = 0; t < nthreads; ++t) {
+      free(ws[t].counts); free(ws[t].col); free(ws[t].val); free(ws[t].val32);
+      free(ws[t].absum); free(ws[t].nterms);
+    }
+  free(at_ptr); free(at_k); free(at_v); free(cur); free(row_p); free(ws); free(th);
+  oracle_free(res);
+  return NULL;
+}

@@ -1,0 +1,231 @@
+// C ABI of the engine (include/spgemm_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+
+#include "../../include/spgemm_b200.h"
+#include "engine.h"
+
+struct spgemm_context {
+  sg::Engine eng;
+};
+
+namespace {
+
+int g_verbose = 1;
+
+int copy_in(sg::Engine& E, sg::DevBuf& buf, const void* host, size_t bytes, void** dev) {
+  cudaError_t e = buf.ensure(bytes ? bytes : 16);
+  if (e != cudaSuccess) return E.cuda_fail(e, "alloc staging buffer");
+  if (bytes) {
+    e = cudaMemcpyAsync(buf.ptr, host, bytes, cudaMemcpyHostToDevice, E.stream());
+    if (e != cudaSuccess) return E.cuda_fail(e, "copy input to device");
+  }
+  *dev = buf.ptr;
+  return SPGEMM_OK;
+}
+
+// Stage a host cm into device buffers 3*slot .. 3*slot+2.
+int stage_matrix(sg::Engine& E, const cm& H, int slot, cm* D) {
+  if (!H.ptr || (H.nnz > 0 && (!H.idx || !H.val)))
+    return E.fail(SPGEMM_ERR_INVALID, "null host array");
+  if (H.nnz < 0 || H.num_rows < 0 || H.num_cols < 0)
+    return E.fail(SPGEMM_ERR_INVALID, "negative dimension or nnz");
+  const size_t nptr = (size_t)(H.type == COL_MAJOR ? H.num_cols : H.num_rows) + 1;
+  *D = H;
+  void* p = nullptr;
+  if (int r = copy_in(E, E.stage(3 * slot), H.ptr, sizeof(int) * nptr, &p)) return r;
+  D->ptr = static_cast<int*>(p);
+  if (int r = copy_in(E, E.stage(3 * slot + 1), H.idx, sizeof(int) * (size_t)H.nnz, &p)) return r;
+  D->idx = static_cast<int*>(p);
+  if (int r = copy_in(E, E.stage(3 * slot + 2), H.val, sizeof(float) * (size_t)H.nnz, &p)) return r;
+  D->val = static_cast<float*>(p);
+  return SPGEMM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int spgemm_internal_verbose(void) { return g_verbose; }
+
+const char* spgemm_version(void) { return "spgemm_b200 0.1.0 (sm_100a)"; }
+
+const char* spgemm_status_string(int s) {
+  switch (s) {
+    case SPGEMM_OK: return "ok";
+    case SPGEMM_ERR_INVALID: return "invalid argument";
+    case SPGEMM_ERR_CUDA: return "CUDA error";
+    case SPGEMM_ERR_ALLOC: return "allocation failed";
+    case SPGEMM_ERR_OVERFLOW: return "nnz(C) exceeds int32";
+    case SPGEMM_ERR_STATE: return "call out of order";
+    case SPGEMM_ERR_DEVICE: return "device-side check failed";
+    case SPGEMM_ERR_TOO_LARGE: return "size exceeds a documented maximum";
+    default: return "unknown status";
+  }
+}
+
+int spgemm_create(spgemm_handle_t* handle) {
+  if (!handle) return SPGEMM_ERR_INVALID;
+  *handle = nullptr;
+  spgemm_context* c = new (std::nothrow) spgemm_context();
+  if (!c) return SPGEMM_ERR_ALLOC;
+  *handle = c;
+  return SPGEMM_OK;
+}
+
+int spgemm_destroy(spgemm_handle_t handle) {
+  delete handle;
+  return SPGEMM_OK;
+}
+
+int spgemm_set_stream(spgemm_handle_t h, void* stream) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->eng.set_stream(static_cast<cudaStream_t>(stream));
+}
+
+int spgemm_set_precision(spgemm_handle_t h, int precision) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->eng.set_precision(precision);
+}
+
+const char* spgemm_last_error(spgemm_handle_t h) {
+  return h ? h->eng.last_error().c_str() : "null handle";
+}
+
+int spgemm_symbolic(spgemm_handle_t h, cm A, cm B, long long* nnz_c) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->eng.symbolic(A, B, nnz_c);
+}
+
+int spgemm_numeric(spgemm_handle_t h, int* c_rowptr, int* c_colidx, float* c_val) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->eng.numeric(c_rowptr, c_colidx, c_val);
+}
+
+int spgemm_multiply(spgemm_handle_t h, cm A, cm B, cm* C) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->eng.multiply(A, B, C);
+}
+
+int spgemm_get_stats(spgemm_handle_t h, spgemm_stats* out) {
+  if (!h || !out) return SPGEMM_ERR_INVALID;
+  memset(out, 0, sizeof(*out));
+  const sg::Engine& E = h->eng;
+  out->intermediate_products = E.intermediate_products();
+  out->nnz_c = E.nnz_c();
+  for (int b = 0; b < sg::SB_COUNT; ++b) out->rows_per_symbolic_bin[b] = E.sym_bin_rows(b);
+  for (int b = 0; b < sg::NB_COUNT; ++b) out->rows_per_numeric_bin[b] = E.num_bin_rows(b);
+  out->long_row_slices = E.slices();
+  out->kernel_launches = E.launches();
+  return SPGEMM_OK;
+}
+
+int spgemm_multiply_host_to(spgemm_handle_t h, cm A_host, cm B_host, int* c_rowptr,
+                            int* c_colidx, float* c_val, long long capacity,
+                            long long* nnz_c) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  sg::Engine& E = h->eng;
+  cm A, B;
+  if (int r = stage_matrix(E, A_host, 0, &A)) return r;
+  if (int r = stage_matrix(E, B_host, 1, &B)) return r;
+  long long nnz = 0;
+  if (int r = E.symbolic(A, B, &nnz)) return r;
+  if (nnz_c) *nnz_c = nnz;
+  if (nnz > capacity || !c_rowptr || (nnz > 0 && (!c_colidx || !c_val)))
+    return E.fail(SPGEMM_ERR_TOO_LARGE, "output capacity below nnz(C)");
+  cm C;
+  if (int r = E.multiply_numeric_owned(&C)) return r;
+  cudaStream_t s = E.stream();
+  cudaError_t e;
+  e = cudaMemcpyAsync(c_rowptr, C.ptr, sizeof(int) * ((size_t)C.num_rows + 1),
+                      cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && nnz > 0)
+    e = cudaMemcpyAsync(c_colidx, C.idx, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && nnz > 0)
+    e = cudaMemcpyAsync(c_val, C.val, sizeof(float) * (size_t)nnz, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return E.cuda_fail(e, "copy C to host");
+  return SPGEMM_OK;
+}
+
+int spgemm_multiply_host(spgemm_handle_t h, cm A_host, cm B_host, cm* C_host) {
+  if (!h || !C_host) return SPGEMM_ERR_INVALID;
+  sg::Engine& E = h->eng;
+  cm A, B;
+  if (int r = stage_matrix(E, A_host, 0, &A)) return r;
+  if (int r = stage_matrix(E, B_host, 1, &B)) return r;
+  cm C;
+  if (int r = E.multiply(A, B, &C)) return r;
+  cm out;
+  out.num_rows = C.num_rows;
+  out.num_cols = C.num_cols;
+  out.nnz = C.nnz;
+  out.type = ROW_MAJOR;
+  out.ptr = static_cast<int*>(malloc(sizeof(int) * ((size_t)C.num_rows + 1)));
+  out.idx = static_cast<int*>(malloc(sizeof(int) * (size_t)(C.nnz > 0 ? C.nnz : 1)));
+  out.val = static_cast<float*>(malloc(sizeof(float) * (size_t)(C.nnz > 0 ? C.nnz : 1)));
+  if (!out.ptr || !out.idx || !out.val) {
+    free(out.ptr); free(out.idx); free(out.val);
+    return E.fail(SPGEMM_ERR_ALLOC, "host allocation of C failed");
+  }
+  cudaStream_t s = E.stream();
+  cudaError_t e = cudaMemcpyAsync(out.ptr, C.ptr, sizeof(int) * ((size_t)C.num_rows + 1),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && C.nnz > 0)
+    e = cudaMemcpyAsync(out.idx, C.idx, sizeof(int) * (size_t)C.nnz, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && C.nnz > 0)
+    e = cudaMemcpyAsync(out.val, C.val, sizeof(float) * (size_t)C.nnz, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    free(out.ptr); free(out.idx); free(out.val);
+    return E.cuda_fail(e, "copy C to host");
+  }
+  *C_host = out;
+  return SPGEMM_OK;
+}
+
+void spgemm_set_verbose(int verbose) { g_verbose = verbose ? 1 : 0; }
+
+int spgemm_set_profiling(spgemm_handle_t h, int enable) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  h->eng.set_profiling(enable != 0);
+  return SPGEMM_OK;
+}
+
+int spgemm_reset_kernel_times(spgemm_handle_t h) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  h->eng.prof_reset();
+  return SPGEMM_OK;
+}
+
+int spgemm_get_kernel_times(spgemm_handle_t h, char* names, int names_len, double* ms,
+                            long long* launches, int max_kernels) {
+  if (!h || max_kernels < 0) return -SPGEMM_ERR_INVALID;
+  const auto& t = h->eng.prof_ms();
+  const auto& c = h->eng.prof_count();
+  int i = 0;
+  size_t pos = 0;
+  if (names && names_len > 0) names[0] = 0;
+  for (const auto& kv : t) {
+    if (i >= max_kernels) break;
+    if (ms) ms[i] = kv.second;
+    if (launches) {
+      auto it = c.find(kv.first);
+      launches[i] = it == c.end() ? 0 : it->second;
+    }
+    if (names && pos + kv.first.size() + 2 <= (size_t)names_len) {
+      memcpy(names + pos, kv.first.data(), kv.first.size());
+      pos += kv.first.size();
+      names[pos++] = '\n';
+      names[pos] = 0;
+    }
+    ++i;
+  }
+  return i;
+}
+
+}  // extern "C"

@@ -1,0 +1,580 @@
+// Host orchestration of the SpGEMM pipeline (see pipeline.cuh).
+//
+// Reference call chain replaced here (src/main.cu:31-37):
+//   cudaInitGEMM (src/mm.cu:150-193)      -> row analysis: P_i, P
+//   cudaCategorizeGEMM (src/mm.cu:263-286) -> symbolic binning
+//   cudaBinGEMM (src/mm.cu:314-327)        -> symbolic pass per bin
+//   cudaMergeGEMM (src/mm.cu:407-450)      -> numeric pass per bin
+// The reference synchronises after every kernel and copies C back one row at
+// a time; this engine synchronises twice per product (bin counts, nnz(C))
+// and leaves C in device memory.
+#include "engine.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "pipeline.cuh"
+
+namespace sg {
+
+cudaError_t DevBuf::ensure(size_t want) {
+  if (want <= bytes && ptr) return cudaSuccess;
+  if (ptr) { cudaFree(ptr); ptr = nullptr; bytes = 0; }
+  if (want == 0) want = 16;
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) { ptr = nullptr; bytes = 0; return e; }
+  bytes = want;
+  return cudaSuccess;
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+Tuning default_tuning() {
+  Tuning t;
+  t.warp_p_max_sym = 1024;
+  t.warp_p_max_num = 2048;
+  t.long_p_sym = 4096;
+  t.long_o_num = 4096;
+  t.slice_cap = 16384;      // recomputed per product from the shared-memory budget
+  t.slice_cols = 1 << 18;
+  t.sym_window = 1 << 20;
+  return t;
+}
+
+// Dynamic shared memory available to one long-row block.
+static constexpr size_t LONG_SMEM_BUDGET = 220 * 1024;
+static constexpr size_t SEG_SCRATCH_BYTES = sizeof(SegScratch);
+
+Engine::Engine() {
+  tn_ = default_tuning();
+  cudaGetDevice(&device_);
+  int v = 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device_) == cudaSuccess && v > 0)
+    sms_ = v;
+  cudaMallocHost(reinterpret_cast<void**>(&host_counters_), sizeof(DevCounters));
+}
+
+cudaEvent_t Engine::prof_take() {
+  if (!prof_pool_.empty()) {
+    cudaEvent_t e = prof_pool_.back();
+    prof_pool_.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+void Engine::prof_begin(const char* name) {
+  if (!prof_on_) return;
+  cudaEvent_t a = prof_take();
+  cudaEventRecord(a, stream_);
+  prof_open_.push_back(ProfRec{name, a, nullptr});
+}
+
+void Engine::prof_end() {
+  if (!prof_on_ || prof_open_.empty() || prof_open_.back().b) return;
+  cudaEvent_t b = prof_take();
+  cudaEventRecord(b, stream_);
+  prof_open_.back().b = b;
+}
+
+int Engine::prof_collect() {
+  for (ProfRec& r : prof_open_) {
+    if (r.b) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+        prof_ms_[r.name] += ms;
+        prof_count_[r.name] += 1;
+      }
+      prof_pool_.push_back(r.b);
+    }
+    prof_pool_.push_back(r.a);
+  }
+  prof_open_.clear();
+  return 0;
+}
+
+Engine::~Engine() {
+  DevBuf* all[] = {&a_rowptr_, &a_col_, &a_val_, &cursor_, &aoff_, &row_p_, &c_cnt_,
+                   &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
+                   &chunk_cnt_, &slices_buf_, &counters_, &out_rowptr_, &out_col_,
+                   &out_val_};
+  for (DevBuf* b : all) b->release();
+  for (DevBuf& b : stage_) b.release();
+  if (host_counters_) cudaFreeHost(host_counters_);
+  for (ProfRec& r : prof_open_) {
+    if (r.a) cudaEventDestroy(r.a);
+    if (r.b) cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : prof_pool_) cudaEventDestroy(e);
+}
+
+int Engine::fail(int status, const std::string& msg) {
+  err_ = msg;
+  return status;
+}
+
+int Engine::cuda_fail(cudaError_t e, const char* what) {
+  err_ = std::string(what) + ": " + cudaGetErrorString(e);
+  return e == cudaErrorMemoryAllocation ? 3 /*SPGEMM_ERR_ALLOC*/ : 2 /*SPGEMM_ERR_CUDA*/;
+}
+
+int Engine::set_tuning(const Tuning& t) {
+  // numeric long rows read the chunk counts that only symbolic long rows
+  // write, so every numeric long row must have been a symbolic long row
+  if (t.long_o_num < t.long_p_sym) return fail(1, "tuning: long_o_num < long_p_sym");
+  if (t.long_p_sym > 4096 || t.long_o_num > 4096)
+    return fail(1, "tuning: hash bins hold at most 4096 distinct columns");
+  if (t.slice_cols < CHUNK_COLS || t.slice_cols % CHUNK_COLS) return fail(1, "tuning: slice_cols");
+  if (t.sym_window < CHUNK_COLS || t.sym_window % CHUNK_COLS || t.sym_window > (1 << 20))
+    return fail(1, "tuning: sym_window");
+  if (t.warp_p_max_sym < 0 || t.warp_p_max_num < 0) return fail(1, "tuning: warp limits");
+  tn_ = t;
+  return 0;
+}
+
+int Engine::set_stream(cudaStream_t s) {
+  stream_ = s;
+  return 0;
+}
+
+int Engine::set_precision(int p) {
+  if (p != 0 && p != 1) return fail(1, "precision must be 0 (plain) or 1 (compensated)");
+  precision_ = p;
+  return 0;
+}
+
+template <class K>
+cudaError_t Engine::smem_attr(K kernel, size_t bytes) {
+  const void* key = reinterpret_cast<const void*>(kernel);
+  auto it = smem_set_.find(key);
+  if (it != smem_set_.end() && it->second >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)bytes);
+  if (e == cudaSuccess) smem_set_[key] = bytes;
+  return e;
+}
+
+#define SG_CK(call, what)                                  \
+  do {                                                     \
+    cudaError_t e__ = (call);                              \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what);   \
+  } while (0)
+
+#define SG_LAUNCHED(what)                                  \
+  do {                                                     \
+    ++launches_;                                           \
+    prof_end();                                            \
+    cudaError_t e__ = cudaGetLastError();                  \
+    if (e__ != cudaSuccess) return cuda_fail(e__, what);   \
+  } while (0)
+
+static inline int blocks_for(long long work, int per_block, long long cap) {
+  long long b = (work + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > cap) b = cap;
+  return (int)b;
+}
+
+int Engine::check_status(unsigned st) {
+  if (!st) return 0;
+  std::string msg = "device check failed:";
+  if (st & ST_TABLE_FULL) msg += " hash-table-full";
+  if (st & ST_COUNT_MISMATCH) msg += " symbolic/numeric-count-mismatch";
+  if (st & ST_ROW_TOO_LONG) msg += " row-with-2^31-or-more-partial-products";
+  if (st & ST_SLICE_OVERFLOW) msg += " slice-list-overflow";
+  if (st & ST_BAD_INDEX) msg += " index-out-of-range";
+  if (st & ST_UNSORTED) msg += " B-row-not-sorted-by-column";
+  return fail(st & ST_ROW_TOO_LONG ? 7 : ((st & (ST_BAD_INDEX | ST_UNSORTED)) ? 1 : 6), msg);
+}
+
+int Engine::scan_counts(const int* in, int n, long long* out) {
+  const int ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  SG_CK(tiles_.ensure(sizeof(long long) * (size_t)std::max(ntiles, 1)), "alloc scan tiles");
+  long long* tiles = tiles_.as<long long>();
+  long long* total = &counters_.as<DevCounters>()->grand_total;
+  if (ntiles > 0) {
+    prof_begin("k_scan_tiles");
+    k_scan_tiles<<<ntiles, SCAN_THREADS, 0, stream_>>>(in, n, tiles);
+    SG_LAUNCHED("k_scan_tiles");
+  }
+  prof_begin("k_scan_tile_sums");
+  k_scan_tile_sums<<<1, SCAN_THREADS, 0, stream_>>>(tiles, ntiles, total);
+  SG_LAUNCHED("k_scan_tile_sums");
+  prof_begin("k_scan_apply");
+  k_scan_apply<<<std::max(ntiles, 1), SCAN_THREADS, 0, stream_>>>(in, n, tiles, total, out);
+  SG_LAUNCHED("k_scan_apply");
+  return 0;
+}
+
+int Engine::symbolic(const cm& A, const cm& B, long long* nnz_c) {
+  if (int r = analyze(A, B)) return r;
+  return symbolic_pass(nnz_c);
+}
+
+int Engine::analyze(const cm& A, const cm& B) {
+  have_sym_ = false;
+  have_analysis_ = false;
+  if (B.type != ROW_MAJOR) return fail(1, "B must be CSR (type ROW_MAJOR)");
+  if (A.num_rows < 0 || A.num_cols < 0 || B.num_cols < 0 || A.nnz < 0 || B.nnz < 0)
+    return fail(1, "negative dimension or nnz");
+  if (A.num_cols != B.num_rows) return fail(1, "A.num_cols != B.num_rows");
+  if (!A.ptr || !B.ptr) return fail(1, "null pointer array");
+  if ((A.nnz > 0 && (!A.idx || !A.val)) || (B.nnz > 0 && (!B.idx || !B.val)))
+    return fail(1, "null index/value array");
+  m_ = A.num_rows;
+  kdim_ = A.num_cols;
+  n_ = B.num_cols;
+  const int nnz_a = A.nnz;
+  const int m = m_;
+
+  SG_CK(counters_.ensure(sizeof(DevCounters)), "alloc counters");
+  DevCounters* dc = counters_.as<DevCounters>();
+  SG_CK(cudaMemsetAsync(dc, 0, sizeof(DevCounters), stream_), "memset counters");
+
+  // ---- validate the operands (sync point 1 reports the result) ----
+  {
+    const int vb = blocks_for((long long)std::max(kdim_, m) * 32, 256, (long long)sms_ * 16);
+    prof_begin("k_validate");
+    k_validate<<<vb, 256, 0, stream_>>>(B.ptr, kdim_, B.idx, B.nnz, n_, 1, &dc->status);
+    SG_LAUNCHED("k_validate(B)");
+    prof_begin("k_validate");
+    if (A.type == COL_MAJOR)
+      k_validate<<<vb, 256, 0, stream_>>>(A.ptr, kdim_, A.idx, nnz_a, m, 0, &dc->status);
+    else
+      k_validate<<<vb, 256, 0, stream_>>>(A.ptr, m, A.idx, nnz_a, kdim_, 0, &dc->status);
+    SG_LAUNCHED("k_validate(A)");
+    // Later kernels index with these values, so stop here if they are bad.
+    SG_CK(cudaMemcpyAsync(&host_counters_->status, &dc->status, sizeof(unsigned),
+                          cudaMemcpyDeviceToHost, stream_), "read status");
+    SG_CK(cudaStreamSynchronize(stream_), "sync after validation");
+    if (int r = check_status(host_counters_->status)) return r;
+  }
+
+  // ---- A in CSR ----
+  const int* a_rowptr;
+  const int* a_col;
+  const float* a_val;
+  SG_CK(c_cnt_.ensure(sizeof(int) * (size_t)std::max(m, 1)), "alloc c_cnt");
+  SG_CK(c_rowptr64_.ensure(sizeof(long long) * ((size_t)m + 1)), "alloc c_rowptr64");
+  if (A.type == COL_MAJOR) {
+    SG_CK(a_rowptr_.ensure(sizeof(int) * ((size_t)m + 1)), "alloc a_rowptr");
+    SG_CK(cursor_.ensure(sizeof(int) * ((size_t)m + 1)), "alloc cursor");
+    SG_CK(a_col_.ensure(sizeof(int) * (size_t)std::max(nnz_a, 1)), "alloc a_col");
+    SG_CK(a_val_.ensure(sizeof(float) * (size_t)std::max(nnz_a, 1)), "alloc a_val");
+    int* cnt = c_cnt_.as<int>();
+    SG_CK(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)std::max(m, 1), stream_), "memset cnt");
+    if (nnz_a > 0) {
+      prof_begin("k_transpose_hist");
+      k_transpose_hist<<<blocks_for(nnz_a, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+          A.idx, nnz_a, m, cnt, &dc->status);
+      SG_LAUNCHED("k_transpose_hist");
+    }
+    if (int r = scan_counts(cnt, m, c_rowptr64_.as<long long>())) return r;
+    prof_begin("k_rowptr_i64_to_i32_shift");
+    k_rowptr_i64_to_i32_shift<<<blocks_for(m + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+        c_rowptr64_.as<long long>(), m + 1, a_rowptr_.as<int>(), cursor_.as<int>());
+    SG_LAUNCHED("k_rowptr_i64_to_i32_shift");
+    if (nnz_a > 0) {
+      prof_begin("k_transpose_scatter");
+      k_transpose_scatter<<<blocks_for(nnz_a, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+          A.ptr, A.idx, A.val, kdim_, nnz_a, m, cursor_.as<int>(), a_col_.as<int>(),
+          a_val_.as<float>());
+      SG_LAUNCHED("k_transpose_scatter");
+    }
+    a_rowptr = a_rowptr_.as<int>();
+    a_col = a_col_.as<int>();
+    a_val = a_val_.as<float>();
+  } else {
+    a_rowptr = A.ptr;
+    a_col = A.idx;
+    a_val = A.val;
+  }
+
+  // ---- row analysis ----
+  SG_CK(aoff_.ensure(sizeof(int) * (size_t)std::max(nnz_a, 1)), "alloc aoff");
+  SG_CK(row_p_.ensure(sizeof(long long) * (size_t)std::max(m, 1)), "alloc row_p");
+  SG_CK(sym_rows_.ensure(sizeof(int) * (size_t)SB_COUNT * std::max(m, 1)), "alloc sym_rows");
+  op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_};
+  if (m > 0) {
+    prof_begin("k_row_analysis");
+    k_row_analysis<<<(m + RA_ROWS - 1) / RA_ROWS, RA_THREADS, 0, stream_>>>(
+        op_, aoff_.as<int>(), row_p_.as<long long>(), c_cnt_.as<int>(), dc->sym_count,
+        sym_rows_.as<int>(), &dc->p_total, &dc->status, tn_);
+    SG_LAUNCHED("k_row_analysis");
+  }
+  SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
+        "read counters");
+  SG_CK(cudaStreamSynchronize(stream_), "sync after row analysis");
+  if (int r = check_status(host_counters_->status)) return r;
+  p_total_ = (long long)host_counters_->p_total;
+  for (int b = 0; b < SB_COUNT; ++b) sym_counts_[b] = host_counters_->sym_count[b];
+  n_long_sym_ = sym_counts_[SB_LONG];
+  n_chunks_ = (n_ + CHUNK_COLS - 1) / CHUNK_COLS;
+  have_analysis_ = true;
+  return 0;
+}
+
+int Engine::symbolic_pass(long long* nnz_c) {
+  if (!have_analysis_) return fail(5, "symbolic pass called before row analysis");
+  have_sym_ = false;
+  const int m = m_;
+  DevCounters* dc = counters_.as<DevCounters>();
+
+  // ---- symbolic pass ----
+  if (n_long_sym_ > 0) {
+    SG_CK(long_slot_.ensure(sizeof(int) * (size_t)std::max(m, 1)), "alloc long_slot");
+    SG_CK(chunk_cnt_.ensure(sizeof(int) * (size_t)n_long_sym_ * std::max(n_chunks_, 1)),
+          "alloc chunk counts");
+  }
+  if (int r = launch_symbolic_bins()) return r;
+
+  // ---- row pointers + numeric binning ----
+  if (int r = scan_counts(c_cnt_.as<int>(), m, c_rowptr64_.as<long long>())) return r;
+  SG_CK(num_rows_.ensure(sizeof(int) * (size_t)NB_COUNT * std::max(m, 1)), "alloc num_rows");
+  const long long slice_cap_rows = (long long)n_long_sym_ * std::max(n_chunks_, 1);
+  SG_CK(slices_buf_.ensure(sizeof(Slice) * (size_t)std::max(slice_cap_rows, 1ll)), "alloc slices");
+  // long-slice output capacity from the shared-memory budget
+  Tuning tr = tn_;
+  {
+    const size_t vb = precision_ == 1 ? 8 : 4;
+    const int width = std::min(n_, tr.slice_cols);
+    const size_t dir_bytes = (size_t)((width + 31) / 32) * sizeof(uint2);
+    const size_t fixed = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + dir_bytes;
+    long long cap = (long long)((LONG_SMEM_BUDGET - fixed) / vb);
+    cap = std::min<long long>(cap, 1 << 20);
+    tr.slice_cap = (int)cap;
+    tn_run_slice_cap_ = tr.slice_cap;
+  }
+  if (m > 0) {
+    prof_begin("k_num_bin");
+    k_num_bin<<<(m + NBIN_THREADS - 1) / NBIN_THREADS, NBIN_THREADS, 0, stream_>>>(
+        m, n_, c_cnt_.as<int>(), row_p_.as<long long>(), c_rowptr64_.as<long long>(),
+        dc->num_count, num_rows_.as<int>(), long_slot_.as<int>(), chunk_cnt_.as<int>(),
+        n_chunks_, slices_buf_.as<Slice>(), &dc->slice_count, (int)slice_cap_rows,
+        &dc->status, tr);
+    SG_LAUNCHED("k_num_bin");
+  }
+  SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
+        "read counters");
+  SG_CK(cudaStreamSynchronize(stream_), "sync after symbolic pass");
+  if (int r = check_status(host_counters_->status)) return r;
+  nnz_c_ = host_counters_->grand_total;
+  for (int b = 0; b < NB_COUNT; ++b) num_counts_[b] = host_counters_->num_count[b];
+  nslices_ = host_counters_->slice_count;
+  if (nnz_c_ > 2147483647ll)
+    return fail(4, "nnz(C) = " + std::to_string(nnz_c_) + " exceeds the int32 range of cm");
+  if (nnz_c) *nnz_c = nnz_c_;
+  have_sym_ = true;
+  return 0;
+}
+
+int Engine::launch_symbolic_bins() {
+  const Operands op = op_;
+  unsigned* status = &counters_.as<DevCounters>()->status;
+  const int m = m_;
+  int* c_cnt = c_cnt_.as<int>();
+  const long long* row_p = row_p_.as<long long>();
+  const int* rows = sym_rows_.as<int>();
+  constexpr int WPB = SW_THREADS / 32;
+  // long rows first: they are the heaviest work items
+  if (sym_counts_[SB_LONG] > 0) {
+    const int win = std::min(n_, tn_.sym_window);
+    const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)((win + 31) / 32) * 4;
+    SG_CK(smem_attr(k_sym_long, smem), "smem attr k_sym_long");
+    const int cnt = sym_counts_[SB_LONG];
+    prof_begin("k_sym_long");
+    k_sym_long<<<blocks_for(cnt, 1, (long long)sms_ * 2), LONG_THREADS, smem, stream_>>>(
+        op, rows + (size_t)SB_LONG * m, cnt, row_p, c_cnt, long_slot_.as<int>(),
+        chunk_cnt_.as<int>(), n_chunks_, status, tn_);
+    SG_LAUNCHED("k_sym_long");
+  }
+#define SG_SYM_WARP(L)                                                                    \
+  {                                                                                        \
+    const int b = L - 6, cnt = sym_counts_[b];                                             \
+    if (cnt > 0) {                                                                         \
+      const size_t smem = WPB * ((size_t(1) << L) * 4 + SEG_SCRATCH_BYTES);                \
+      SG_CK(smem_attr(k_sym_warp<L>, smem), "smem attr k_sym_warp");                       \
+      prof_begin("k_sym_warp<" #L ">");                                                            \
+      k_sym_warp<L><<<blocks_for(cnt, WPB, (long long)sms_ * 8), SW_THREADS, smem, stream_>>>( \
+          op, rows + (size_t)b * m, cnt, c_cnt, status);                                   \
+      SG_LAUNCHED("k_sym_warp");                                                           \
+    }                                                                                      \
+  }
+  SG_SYM_WARP(6) SG_SYM_WARP(7) SG_SYM_WARP(8) SG_SYM_WARP(9) SG_SYM_WARP(10)
+#undef SG_SYM_WARP
+#define SG_SYM_BLOCK(L, NT)                                                               \
+  {                                                                                        \
+    const int b = L - 11 + 5, cnt = sym_counts_[b];                                        \
+    if (cnt > 0) {                                                                         \
+      const size_t smem = (size_t(1) << L) * 4 + (NT / 32) * SEG_SCRATCH_BYTES;            \
+      SG_CK(smem_attr(k_sym_block<L, NT>, smem), "smem attr k_sym_block");                 \
+      prof_begin("k_sym_block<" #L ">");                                                       \
+      k_sym_block<L, NT><<<blocks_for(cnt, 1, (long long)sms_ * 8), NT, smem, stream_>>>(  \
+          op, rows + (size_t)b * m, cnt, row_p, c_cnt, status);                            \
+      SG_LAUNCHED("k_sym_block");                                                          \
+    }                                                                                      \
+  }
+  SG_SYM_BLOCK(11, 256) SG_SYM_BLOCK(12, 256) SG_SYM_BLOCK(13, 256)
+#undef SG_SYM_BLOCK
+  return 0;
+}
+
+template <int MODE>
+static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, int m,
+                               const int* counts, int nslices, const Slice* slices,
+                               const int* nslices_dev, const long long* row_p,
+                               const long long* c_rowptr, int* c_col, float* c_val,
+                               unsigned* status, cudaStream_t stream, int sms, int n,
+                               int slice_cols, int slice_cap, long long& launches);
+
+int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
+  if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
+  if (!c_rowptr || (nnz_c_ > 0 && (!c_col || !c_val))) return fail(1, "null output pointer");
+  if (int r = launch_numeric_bins(c_col, c_val)) return r;
+  prof_begin("k_rowptr_to_i32");
+  k_rowptr_to_i32<<<blocks_for(m_ + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+      c_rowptr64_.as<long long>(), m_ + 1, c_rowptr);
+  SG_LAUNCHED("k_rowptr_to_i32");
+  DevCounters* dc = counters_.as<DevCounters>();
+  SG_CK(cudaMemcpyAsync(&host_counters_->status, &dc->status, sizeof(unsigned),
+                        cudaMemcpyDeviceToHost, stream_),
+        "read status");
+  SG_CK(cudaStreamSynchronize(stream_), "sync after numeric pass");
+  prof_collect();
+  return check_status(host_counters_->status);
+}
+
+int Engine::launch_numeric_bins(int* c_col, float* c_val) {
+  DevCounters* dc = counters_.as<DevCounters>();
+  if (precision_ == 0)
+    return launch_numeric_impl<0>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
+                                  slices_buf_.as<Slice>(), &dc->slice_count,
+                                  row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
+                                  c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
+                                  tn_run_slice_cap_, launches_);
+  return launch_numeric_impl<1>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
+                                slices_buf_.as<Slice>(), &dc->slice_count,
+                                row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
+                                c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
+                                tn_run_slice_cap_, launches_);
+}
+
+template <class K>
+static cudaError_t set_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+#define SG_CKE(call, what)                                  \
+  do {                                                      \
+    cudaError_t e__ = (call);                               \
+    if (e__ != cudaSuccess) return E.cuda_fail(e__, what);  \
+  } while (0)
+#define SG_LAUNCHED_E(what)                                 \
+  do {                                                      \
+    ++launches;                                             \
+    E.prof_end();                                           \
+    cudaError_t e__ = cudaGetLastError();                   \
+    if (e__ != cudaSuccess) return E.cuda_fail(e__, what);  \
+  } while (0)
+
+template <int MODE>
+static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, int m,
+                               const int* counts, int nslices, const Slice* slices,
+                               const int* nslices_dev, const long long* row_p,
+                               const long long* c_rowptr, int* c_col, float* c_val,
+                               unsigned* status, cudaStream_t stream, int sms, int n,
+                               int slice_cols, int slice_cap, long long& launches) {
+  constexpr int WPB = SW_THREADS / 32;
+  constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
+  if (nslices > 0) {
+    const int width = std::min(n, slice_cols);
+    const int dir_words = (width + 31) / 32;
+    const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES +
+                        (size_t)dir_words * sizeof(uint2) + (size_t)slice_cap * (MODE ? 8 : 4);
+    SG_CKE(set_smem(k_num_long<MODE>, smem), "smem attr k_num_long");
+    E.prof_begin("k_num_long");
+    k_num_long<MODE><<<blocks_for(nslices, 1, (long long)sms * 2), LONG_THREADS, smem, stream>>>(
+        op, slices, nslices, row_p, dir_words, slice_cap, c_col, c_val, status);
+    SG_LAUNCHED_E("k_num_long");
+  }
+#define SG_NUM_WARP(L)                                                                       \
+  {                                                                                           \
+    const int b = L - 6, cnt = counts[b];                                                     \
+    if (cnt > 0) {                                                                            \
+      const size_t smem = WPB * ((size_t(1) << L) * (VB + 4) + SEG_SCRATCH_BYTES);            \
+      SG_CKE(set_smem(k_num_warp<L, MODE>, smem), "smem attr k_num_warp");                    \
+      E.prof_begin("k_num_warp<" #L ">");                                                          \
+      k_num_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms * 8), SW_THREADS, smem,       \
+                            stream>>>(op, rows + (size_t)b * m, cnt, c_rowptr, c_col, c_val,  \
+                                      status);                                                \
+      SG_LAUNCHED_E("k_num_warp");                                                            \
+    }                                                                                         \
+  }
+  SG_NUM_WARP(6) SG_NUM_WARP(7) SG_NUM_WARP(8) SG_NUM_WARP(9)
+#undef SG_NUM_WARP
+#define SG_NUM_BLOCK(L, NT)                                                                  \
+  {                                                                                           \
+    const int b = L - 10 + 4, cnt = counts[b];                                                \
+    if (cnt > 0) {                                                                            \
+      const size_t smem = (size_t(1) << L) * (VB + 4) + (NT / 32) * SEG_SCRATCH_BYTES;        \
+      SG_CKE(set_smem(k_num_block<L, NT, MODE>, smem), "smem attr k_num_block");              \
+      E.prof_begin("k_num_block<" #L ">");                                                         \
+      k_num_block<L, NT, MODE><<<blocks_for(cnt, 1, (long long)sms * 8), NT, smem, stream>>>( \
+          op, rows + (size_t)b * m, cnt, row_p, c_rowptr, c_col, c_val, status);              \
+      SG_LAUNCHED_E("k_num_block");                                                           \
+    }                                                                                         \
+  }
+  SG_NUM_BLOCK(10, 256) SG_NUM_BLOCK(11, 256) SG_NUM_BLOCK(12, 512) SG_NUM_BLOCK(13, 512)
+#undef SG_NUM_BLOCK
+  return 0;
+}
+
+int Engine::multiply(const cm& A, const cm& B, cm* C_dev) {
+  long long nnz = 0;
+  if (int r = symbolic(A, B, &nnz)) return r;
+  return multiply_numeric_owned(C_dev);
+}
+
+int Engine::multiply_numeric_owned(cm* C_dev) {
+  if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
+  const long long nnz = nnz_c_;
+  SG_CK(out_rowptr_.ensure(sizeof(int) * ((size_t)m_ + 1)), "alloc C row pointers");
+  SG_CK(out_col_.ensure(sizeof(int) * (size_t)std::max(nnz, 1ll)), "alloc C columns");
+  SG_CK(out_val_.ensure(sizeof(float) * (size_t)std::max(nnz, 1ll)), "alloc C values");
+  if (int r = numeric(out_rowptr_.as<int>(), out_col_.as<int>(), out_val_.as<float>())) return r;
+  if (C_dev) {
+    C_dev->ptr = out_rowptr_.as<int>();
+    C_dev->idx = out_col_.as<int>();
+    C_dev->val = out_val_.as<float>();
+    C_dev->nnz = (int)nnz;
+    C_dev->num_rows = m_;
+    C_dev->num_cols = n_;
+    C_dev->type = ROW_MAJOR;
+  }
+  return 0;
+}
+
+cudaError_t scan_counts_to_ptr32(const int* cnt, int n, int* ptr, DevBuf& tmp,
+                                 long long* total_dev, cudaStream_t s) {
+  const int ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  const size_t tiles_bytes = sizeof(long long) * (size_t)std::max(ntiles, 1);
+  const size_t ptr64_bytes = sizeof(long long) * ((size_t)n + 1);
+  cudaError_t e = tmp.ensure(tiles_bytes + ptr64_bytes);
+  if (e != cudaSuccess) return e;
+  long long* tiles = tmp.as<long long>();
+  long long* ptr64 = tiles + std::max(ntiles, 1);
+  if (ntiles > 0) k_scan_tiles<<<ntiles, SCAN_THREADS, 0, s>>>(cnt, n, tiles);
+  k_scan_tile_sums<<<1, SCAN_THREADS, 0, s>>>(tiles, ntiles, total_dev);
+  k_scan_apply<<<std::max(ntiles, 1), SCAN_THREADS, 0, s>>>(cnt, n, tiles, total_dev, ptr64);
+  k_rowptr_to_i32<<<blocks_for(n + 1, 256, 4096), 256, 0, s>>>(ptr64, n + 1, ptr);
+  return cudaGetLastError();
+}
+
+}  // namespace sg

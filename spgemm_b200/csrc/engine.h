@@ -1,0 +1,148 @@
+// Host orchestration of the SpGEMM pipeline: workspace, bin scheduling,
+// synchronisation points and error capture. One Engine per spgemm handle.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/cm.h"
+#include "kernels.cuh"
+
+namespace sg {
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t want);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Device-side counters, reset once per product and read back at the two
+// synchronisation points.
+struct DevCounters {
+  int sym_count[16];
+  int num_count[16];
+  int slice_count;
+  unsigned status;
+  unsigned long long p_total;
+  long long grand_total;
+};
+
+class Engine {
+ public:
+  Engine();
+  ~Engine();
+
+  int set_stream(cudaStream_t s);
+  int set_precision(int p);
+  // Rejects tunings that break the kernels' invariants (returns nonzero).
+  int set_tuning(const Tuning& t);
+  const Tuning& tuning() const { return tn_; }
+
+  // Phase 1. A: COL_MAJOR (CSC) or ROW_MAJOR (CSR); B: ROW_MAJOR. Device
+  // pointers. Synchronises the stream twice (bin counts, then nnz(C)).
+  int symbolic(const cm& A, const cm& B, long long* nnz_c);
+  // symbolic() in two stages (used by the mm.h shims): analyze() converts A,
+  // computes P_i and the bins (first sync); symbolic_pass() computes the
+  // exact row counts, row pointers and numeric bins (second sync).
+  int analyze(const cm& A, const cm& B);
+  int symbolic_pass(long long* nnz_c);
+  // Phase 2 into caller-provided device buffers; synchronises once to
+  // check the status word.
+  int numeric(int* c_rowptr, int* c_col, float* c_val);
+  // Both phases into engine-owned output buffers.
+  int multiply(const cm& A, const cm& B, cm* C_dev);
+  // Numeric pass of the current symbolic result into engine-owned buffers.
+  int multiply_numeric_owned(cm* C_dev);
+
+  const std::string& last_error() const { return err_; }
+  long long launches() const { return launches_; }
+  long long intermediate_products() const { return p_total_; }
+  long long nnz_c() const { return nnz_c_; }
+  int m() const { return m_; }
+  int n() const { return n_; }
+  int sym_bin_rows(int b) const { return sym_counts_[b]; }
+  int num_bin_rows(int b) const { return num_counts_[b]; }
+  int slices() const { return nslices_; }
+  cudaStream_t stream() const { return stream_; }
+  int precision() const { return precision_; }
+  // Device buffers of the last multiply() output.
+  int* out_rowptr() const { return out_rowptr_.as<int>(); }
+  int* out_col() const { return out_col_.as<int>(); }
+  float* out_val() const { return out_val_.as<float>(); }
+  // Staging buffers for the host-buffer entry points.
+  DevBuf& stage(int i) { return stage_[i]; }
+
+  // Optional per-kernel timing with CUDA events recorded on the engine's
+  // stream around every launch; accumulated per kernel name.
+  void set_profiling(bool on) { prof_on_ = on; }
+  void prof_begin(const char* name);
+  void prof_end();
+  int prof_collect();  // after a stream sync: fold finished events into totals
+  void prof_reset() { prof_ms_.clear(); prof_count_.clear(); }
+  const std::map<std::string, double>& prof_ms() const { return prof_ms_; }
+  const std::map<std::string, long long>& prof_count() const { return prof_count_; }
+
+  int fail(int status, const std::string& msg);
+  int cuda_fail(cudaError_t e, const char* what);
+
+ private:
+  int launch_symbolic_bins();
+  int launch_numeric_bins(int* c_col, float* c_val);
+  int scan_counts(const int* in, int n, long long* out);
+  int check_status(unsigned st);
+  template <class K> cudaError_t smem_attr(K kernel, size_t bytes);
+
+  cudaStream_t stream_ = nullptr;
+  int device_ = 0;
+  int sms_ = 148;
+  int precision_ = 0;
+  Tuning tn_;
+  std::string err_;
+  long long launches_ = 0;
+  std::unordered_map<const void*, size_t> smem_set_;
+
+  // current product
+  bool have_sym_ = false;
+  int m_ = 0, kdim_ = 0, n_ = 0, n_chunks_ = 0;
+  long long p_total_ = 0, nnz_c_ = 0;
+  int sym_counts_[16] = {0};
+  int num_counts_[16] = {0};
+  int nslices_ = 0;
+  int n_long_sym_ = 0;
+  int tn_run_slice_cap_ = 0;
+  bool have_analysis_ = false;
+  Operands op_{};
+
+  DevBuf a_rowptr_, a_col_, a_val_, cursor_, aoff_;
+  DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
+  DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_;
+  DevBuf counters_;
+  DevBuf out_rowptr_, out_col_, out_val_;
+  DevBuf stage_[6];
+  DevCounters* host_counters_ = nullptr;  // pinned
+
+  bool prof_on_ = false;
+  struct ProfRec { std::string name; cudaEvent_t a, b; };
+  std::vector<ProfRec> prof_open_;
+  std::vector<cudaEvent_t> prof_pool_;
+  std::map<std::string, double> prof_ms_;
+  std::map<std::string, long long> prof_count_;
+  const char* prof_pending_ = nullptr;
+  cudaEvent_t prof_take();
+};
+
+Tuning default_tuning();
+
+// Exclusive scan of n int32 counts into n+1 int32 pointers on `stream`.
+// `tmp` is scratch (grown as needed); `total_dev` receives the sum (int64).
+cudaError_t scan_counts_to_ptr32(const int* cnt, int n, int* ptr, DevBuf& tmp,
+                                 long long* total_dev, cudaStream_t stream);
+
+}  // namespace sg

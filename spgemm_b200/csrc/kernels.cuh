@@ -1,0 +1,439 @@
+// sm_100a kernels of the SpGEMM pipeline C = A * B.
+//
+// The reference expands the outer product A(:,k) * B(k,:) of every k into
+// per-row buckets of C (src/mm.cu:288-312, "binGEMM") and merges each bucket
+// with a dense accumulator (src/mm.cu:366-404, "mergeGEMM"). Materialising the
+// buckets costs 8 bytes of HBM write + read per partial product. Here the
+// same partials are generated bucket by bucket instead: the row i bucket is
+// sum_k A(i,k) * B(k,:), so each C row is expanded and merged in on-chip
+// memory by one warp, one block, or (for long rows) several blocks that
+// each own a column slice. Partials never touch HBM.
+//
+// Pipeline (kernel names):
+//   k_transpose_hist / k_transpose_scatter  A CSC -> CSR (row-wise expansion)
+//   k_row_analysis    P_i per row, flattened offsets, symbolic binning
+//   k_sym_warp/block  exact nnz of short/mid rows via shared-memory hashing
+//   k_sym_long        exact nnz of long rows via a shared-memory bitmap
+//   k_scan_*          row pointers of C
+//   k_num_bin         numeric binning + column slicing of long rows
+//   k_num_warp/block  numeric hash merge + bitonic sort -> sorted CSR rows
+//   k_num_long        numeric bitmap-rank merge (a counting sort on the
+//                     column) -> sorted CSR slices
+#pragma once
+
+#include "common.cuh"
+
+namespace sg {
+
+// ---------------------------------------------------------------------------
+// Operands and tuning
+// ---------------------------------------------------------------------------
+
+struct Operands {
+  const int* __restrict__ a_rowptr;  // A in CSR (m + 1)
+  const int* __restrict__ a_col;     // k index of each A entry
+  const float* __restrict__ a_val;
+  const int* __restrict__ aoff;      // flattened offset of each A entry in its row
+  const int* __restrict__ b_rowptr;  // B in CSR (kdim + 1)
+  const int* __restrict__ b_col;
+  const float* __restrict__ b_val;
+  int m, kdim, n;
+};
+
+// Symbolic bins: 0..4 warp-per-row hash (2^6..2^10 slots), 5..7 block-per-row
+// hash (2^11..2^13 slots), 8 long rows (bitmap).
+constexpr int SB_COUNT = 9;
+constexpr int SB_LONG = 8;
+// Numeric bins: 0..3 warp-per-row (2^6..2^9 slots), 4..7 block-per-row
+// (2^10..2^13 slots), 8 long rows (column slices).
+constexpr int NB_COUNT = 9;
+constexpr int NB_LONG = 8;
+
+constexpr int CHUNK_COLS = 2048;               // column granularity of slicing
+constexpr int CHUNK_WORDS = CHUNK_COLS / 32;
+constexpr long long FP64_ROW_PARTIALS = 4096;  // compensated mode: FP64 above this
+
+struct Tuning {
+  int warp_p_max_sym;   // symbolic: warp-per-row only when P_i <= this
+  int warp_p_max_num;   // numeric: warp-per-row only when P_i <= this
+  int long_p_sym;       // symbolic: bitmap path when P_i > this
+  int long_o_num;       // numeric: slice path when nnz_i > this (>= long_p_sym)
+  int slice_cap;        // max outputs of one numeric long slice
+  int slice_cols;       // max columns of one numeric long slice (multiple of 2048)
+  int sym_window;       // columns per symbolic bitmap window (multiple of 2048)
+};
+
+__host__ __device__ inline int ceil_log2_ll(long long v) {
+  int r = 0;
+  while ((1ll << r) < v) ++r;
+  return r;
+}
+
+__host__ __device__ inline int sym_bin_of(long long p, int n, const Tuning& t) {
+  if (p <= 0) return -1;
+  if (p > t.long_p_sym) return SB_LONG;
+  long long u = p < n ? p : n;
+  int lg = ceil_log2_ll(2 * u);
+  if (lg < 6) lg = 6;
+  if (p <= t.warp_p_max_sym && lg <= 10) return lg - 6;
+  if (lg < 11) lg = 11;
+  return lg - 11 + 5;  // lg <= 13 because u <= long_p_sym <= 4096
+}
+
+__host__ __device__ inline int num_bin_of(int o, long long p, const Tuning& t) {
+  if (o <= 0) return -1;
+  if (o > t.long_o_num) return NB_LONG;
+  int lg = ceil_log2_ll(2ll * o);
+  if (lg < 6) lg = 6;
+  if (p <= t.warp_p_max_num && lg <= 9) return lg - 6;
+  if (lg < 10) lg = 10;
+  return lg - 10 + 4;  // lg <= 13 because o <= long_o_num <= 4096
+}
+
+// One column slice of a long row for the numeric pass.
+struct Slice {
+  long long out;  // first output position in C
+  int row;
+  int lo, hi;     // columns [lo, hi)
+  int cnt;        // outputs in the slice
+};
+
+// ---------------------------------------------------------------------------
+// Expansion primitives
+// ---------------------------------------------------------------------------
+
+// Per-warp staging area used to compact non-empty segments to the front.
+struct SegScratch {
+  int bstart[32];
+  int len[32];
+  float a[32];
+};
+
+// Move the lanes with len > 0 to lanes 0..cnt-1 (order preserved).
+__device__ __forceinline__ int compact_segments(int& bstart, int& len, float& a,
+                                                SegScratch* sc) {
+  const int lane = lane_id();
+  const unsigned m = __ballot_sync(FULL, len > 0);
+  const int cnt = __popc(m);
+  if (m == (cnt == 32 ? FULL : ((1u << cnt) - 1u))) return cnt;  // already a prefix
+  const int r = __popc(m & ((1u << lane) - 1u));
+  if (len > 0) { sc->bstart[r] = bstart; sc->len[r] = len; sc->a[r] = a; }
+  __syncwarp();
+  if (lane < cnt) { bstart = sc->bstart[lane]; len = sc->len[lane]; a = sc->a[lane]; }
+  else { len = 0; }
+  __syncwarp();
+  return cnt;
+}
+
+// Generate every partial product of the (<= 32) compacted segments held by
+// the warp: lane j < cnt holds B positions [bstart, bstart + len) to be
+// scaled by a. The segments are laid end to end and walked 32 products at a
+// time, so lanes stay busy whatever the segment lengths. The owner of each
+// product is found from the OR of segment-start bits in the current window
+// (redux.sync) and a popcount -- O(1) per product, no search.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void run_segments(int cnt, int bstart, int len, float a,
+                                             const int* __restrict__ b_col,
+                                             const float* __restrict__ b_val, F& f) {
+  const int lane = lane_id();
+  if (lane >= cnt) len = 0;
+  const int incl = warp_incl_scan(len);
+  const int total = __shfl_sync(FULL, incl, 31);
+  const int s = incl - len;
+  int nbefore = 0;
+  for (int base = 0; base < total; base += 32) {
+    const unsigned bit =
+        (len > 0 && s >= base && s < base + 32) ? (1u << (s - base)) : 0u;
+    const unsigned starts = __reduce_or_sync(FULL, bit);
+    const int owner = nbefore + __popc(starts & (FULL >> (31 - lane))) - 1;
+    nbefore += __popc(starts);
+    const int ob = __shfl_sync(FULL, bstart, owner);
+    const int os = __shfl_sync(FULL, s, owner);
+    const float oa = __shfl_sync(FULL, a, owner);
+    const int fp = base + lane;
+    if (fp < total) {
+      const int pos = ob + (fp - os);
+      const int col = __ldg(b_col + pos);
+      const float bv = NEED_VAL ? __ldg(b_val + pos) : 0.f;
+      f(col, oa, bv);
+    }
+  }
+}
+
+// Whole row of A, one warp.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_expand_row(const Operands& op, int rs, int re,
+                                                F& f, SegScratch* sc) {
+  const int lane = lane_id();
+  for (int base = rs; base < re; base += 32) {
+    const int j = base + lane;
+    int bstart = 0, len = 0;
+    float a = 0.f;
+    if (j < re) {
+      const int k = __ldg(op.a_col + j);
+      a = __ldg(op.a_val + j);
+      bstart = __ldg(op.b_rowptr + k);
+      len = __ldg(op.b_rowptr + k + 1) - bstart;
+    }
+    const int cnt = compact_segments(bstart, len, a, sc);
+    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+  }
+}
+
+// Products [f0, f1) of the row's flattened product sequence (entries in
+// order, each contributing nnz(B(k,:)) products), one warp. Uses the
+// per-entry flattened offsets `aoff` written by k_row_analysis.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_expand_range(const Operands& op, int rs, int re,
+                                                  int f0, int f1, F& f,
+                                                  SegScratch* sc) {
+  const int lane = lane_id();
+  // Last entry whose offset is <= f0 holds product f0.
+  int lo = rs, hi = re;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(op.aoff + mid) <= f0) lo = mid + 1; else hi = mid;
+  }
+  for (int base = lo - 1; base < re; base += 32) {
+    const int j = base + lane;
+    int bstart = 0, len = 0;
+    float a = 0.f;
+    bool past = true;
+    if (j < re) {
+      const int off = __ldg(op.aoff + j);
+      past = off >= f1;
+      if (!past) {
+        const int k = __ldg(op.a_col + j);
+        const int bs = __ldg(op.b_rowptr + k);
+        const int bl = __ldg(op.b_rowptr + k + 1) - bs;
+        const int l0 = max(off, f0), l1 = min(off + bl, f1);
+        if (l1 > l0) {
+          a = __ldg(op.a_val + j);
+          bstart = bs + (l0 - off);
+          len = l1 - l0;
+        }
+      }
+    }
+    const bool done = __any_sync(FULL, past);
+    const int cnt = compact_segments(bstart, len, a, sc);
+    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+    if (done) break;
+  }
+}
+
+// Entries [jb, min(jb + 32, re)) of a row, each restricted to the columns
+// [clo, chi) of its B row (binary search), one warp.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_expand_restricted(const Operands& op, int jb, int re,
+                                                       int clo, int chi, F& f,
+                                                       SegScratch* sc) {
+  const int lane = lane_id();
+  const int j = jb + lane;
+  int bstart = 0, len = 0;
+  float a = 0.f;
+  if (j < re) {
+    const int k = __ldg(op.a_col + j);
+    const int bs = __ldg(op.b_rowptr + k);
+    const int be = __ldg(op.b_rowptr + k + 1);
+    if (be > bs) {
+      const int first = __ldg(op.b_col + bs), last = __ldg(op.b_col + be - 1);
+      if (first < chi && last >= clo) {
+        const int s0 = first >= clo ? bs : lower_bound_i32(op.b_col, bs, be, clo);
+        const int s1 = last < chi ? be : lower_bound_i32(op.b_col, s0, be, chi);
+        bstart = s0;
+        len = s1 - s0;
+        a = __ldg(op.a_val + j);
+      }
+    }
+  }
+  const int cnt = compact_segments(bstart, len, a, sc);
+  if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+}
+
+// ---------------------------------------------------------------------------
+// Accumulators
+// ---------------------------------------------------------------------------
+
+// Linear-probing insert of `col` into a 2^log2t table; returns the slot or -1
+// (table full: recorded in the status word).
+__device__ __forceinline__ int hash_slot(unsigned* keys, int log2t, unsigned col,
+                                         bool& inserted, unsigned* status) {
+  const unsigned mask = (1u << log2t) - 1u;
+  unsigned h = hash_col(col, log2t);
+  inserted = false;
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const unsigned k = ((volatile unsigned*)keys)[h];
+    if (k == col) return (int)h;
+    if (k == EMPTY_KEY) {
+      const unsigned old = atomicCAS(keys + h, EMPTY_KEY, col);
+      if (old == EMPTY_KEY) { inserted = true; return (int)h; }
+      if (old == col) return (int)h;
+    }
+    h = (h + 1u) & mask;
+  }
+  atomicOr(status, ST_TABLE_FULL);
+  return -1;
+}
+
+struct SymHash {
+  unsigned* keys;
+  int log2t;
+  unsigned* status;
+  int nnew;
+  __device__ __forceinline__ void operator()(int col, float, float) {
+    bool ins;
+    hash_slot(keys, log2t, (unsigned)col, ins, status);
+    nnew += ins;
+  }
+};
+
+// Columns outside [lo, lo + width) cannot occur for validated inputs; the
+// range test keeps a malformed input from writing outside the bitmap.
+struct SymBits {
+  unsigned* bits;
+  int lo;
+  unsigned width;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float, float) {
+    const unsigned c = (unsigned)(col - lo);
+    if (c < width) atomicOr(bits + (c >> 5), 1u << (c & 31));
+    else atomicOr(status, ST_BAD_INDEX);
+  }
+};
+
+struct NumHashPlain {
+  unsigned* keys;
+  float* vals;
+  int log2t;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    bool ins;
+    const int h = hash_slot(keys, log2t, (unsigned)col, ins, status);
+    if (h >= 0) atomicAdd(vals + h, __fmul_rn(a, b));
+  }
+};
+
+// Compensated accumulate of p = a*b into a (sum, comp) pair. The atomic add
+// returns the old sum, and since it rounds to nearest like __fadd_rn, the
+// exact error of that very addition is known locally (TwoSum); it is added
+// to the compensation word together with the product's own rounding error
+// (TwoProduct via FMA). This is Dot2 with the summation order set by the
+// order of atomic arrival.
+__device__ __forceinline__ void twosum_accumulate(float2* slot, float a, float b) {
+  const float p = __fmul_rn(a, b);
+  const float ep = __fmaf_rn(a, b, -p);
+  const float old = atomicAdd(&slot->x, p);
+  const float s = __fadd_rn(old, p);
+  const float e = two_sum_err(old, p, s);
+  atomicAdd(&slot->y, __fadd_rn(e, ep));
+}
+
+struct NumHashTwoSum {
+  unsigned* keys;
+  float2* vals;
+  int log2t;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    bool ins;
+    const int h = hash_slot(keys, log2t, (unsigned)col, ins, status);
+    if (h >= 0) twosum_accumulate(vals + h, a, b);
+  }
+};
+
+struct NumHashF64 {
+  unsigned* keys;
+  double* vals;
+  int log2t;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    bool ins;
+    const int h = hash_slot(keys, log2t, (unsigned)col, ins, status);
+    if (h >= 0) atomicAdd(vals + h, (double)a * (double)b);  // exact product
+  }
+};
+
+// Long rows: directory word w holds the presence bits of columns
+// lo + 32w .. lo + 32w + 31 (.x) and the number of present columns before
+// it (.y), so a column's output slot is .y + popc(.x & lower bits).
+struct LongBits {
+  uint2* dir;
+  int lo;
+  unsigned width;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float, float) {
+    const unsigned c = (unsigned)(col - lo);
+    if (c < width) atomicOr(&dir[c >> 5].x, 1u << (c & 31));
+    else atomicOr(status, ST_BAD_INDEX);
+  }
+};
+
+// Output slot of `col` (only columns whose bit pass 1 set reach here, so
+// the slot is below the slice's output count).
+__device__ __forceinline__ int long_slot(const uint2* dir, int lo, int col) {
+  const unsigned c = (unsigned)(col - lo);
+  const uint2 d = dir[c >> 5];
+  return (int)(d.y + __popc(d.x & ((1u << (c & 31)) - 1u)));
+}
+
+struct LongValPlain {
+  const uint2* dir;
+  float* vals;
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if ((unsigned)(col - lo) < width) atomicAdd(vals + long_slot(dir, lo, col), __fmul_rn(a, b));
+  }
+};
+
+struct LongValF64 {
+  const uint2* dir;
+  double* vals;
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if ((unsigned)(col - lo) < width)
+      atomicAdd(vals + long_slot(dir, lo, col), (double)a * (double)b);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Bitonic sort of a power-of-two key/value array in shared memory
+// ---------------------------------------------------------------------------
+
+struct WarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+struct BlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+template <int N, int NT, class V, class Sync>
+__device__ __forceinline__ void bitonic_sort_kv(unsigned* keys, V* vals, int tid,
+                                                Sync sync) {
+#pragma unroll 1
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll 1
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < N / 2; t += NT) {
+        const int lo = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        const int hi = lo + j;
+        const bool up = (lo & k) == 0;
+        const unsigned kl = keys[lo], kh = keys[hi];
+        if ((kl > kh) == up) {
+          keys[lo] = kh;
+          keys[hi] = kl;
+          const V vl = vals[lo];
+          vals[lo] = vals[hi];
+          vals[hi] = vl;
+        }
+      }
+      sync();
+    }
+  }
+}
+
+__device__ __forceinline__ float finalize_value(float v) { return v; }
+__device__ __forceinline__ float finalize_value(float2 v) { return __fadd_rn(v.x, v.y); }
+__device__ __forceinline__ float finalize_value(double v) { return __double2float_rn(v); }
+
+}  // namespace sg

@@ -1,0 +1,662 @@
+// __global__ kernels of the SpGEMM pipeline (see kernels.cuh for the
+// device primitives they are built from).
+#pragma once
+
+#include "kernels.cuh"
+
+namespace sg {
+
+// ---------------------------------------------------------------------------
+// Input validation
+// ---------------------------------------------------------------------------
+
+// One warp per major index: pointers non-decreasing inside [0, nnz] with
+// ptr[0] == 0 and ptr[n_major] == nnz, minor indices inside [0, n_minor) and,
+// when `sorted` is set, strictly increasing inside each major segment (B's
+// rows must be sorted: the long-row kernels binary-search them). Violations
+// set ST_BAD_INDEX (range) or ST_UNSORTED; nothing is read outside
+// ptr[0..n_major] and idx[0..nnz).
+__global__ void k_validate(const int* __restrict__ ptr, int n_major,
+                           const int* __restrict__ idx, int nnz, int n_minor, int sorted,
+                           unsigned* status) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  if (gw == 0 && lane == 0 && (ptr[0] != 0 || ptr[n_major] != nnz)) atomicOr(status, ST_BAD_INDEX);
+  for (int i = gw; i < n_major; i += nw) {
+    int s = ptr[i], e = ptr[i + 1];
+    if (s > e || s < 0 || e > nnz) {
+      if (lane == 0) atomicOr(status, ST_BAD_INDEX);
+      continue;
+    }
+    for (int q = s + lane; q < e; q += 32) {
+      const int v = idx[q];
+      if ((unsigned)v >= (unsigned)n_minor) atomicOr(status, ST_BAD_INDEX);
+      if (sorted && q > s && idx[q - 1] >= v) atomicOr(status, ST_UNSORTED);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// A: CSC -> CSR
+// ---------------------------------------------------------------------------
+
+// Count entries per row of A. The reference builds A's CSC with the same
+// atomic histogram but never zeroes it first (src/mm.cu:43-63, 89); the
+// caller of this kernel zeroes `cnt`.
+__global__ void k_transpose_hist(const int* __restrict__ rowidx, int nnz, int m,
+                                 int* __restrict__ cnt, unsigned* status) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+       e += gridDim.x * blockDim.x) {
+    const int r = rowidx[e];
+    if ((unsigned)r < (unsigned)m) atomicAdd(cnt + r, 1);
+    else atomicOr(status, ST_BAD_INDEX);
+  }
+}
+
+// Scatter CSC entries into CSR order. cursor[] starts as the CSR row
+// pointers; the entry order inside a row is the atomic arrival order.
+__global__ void k_transpose_scatter(const int* __restrict__ colptr,
+                                    const int* __restrict__ rowidx,
+                                    const float* __restrict__ val, int kdim, int nnz,
+                                    int m, int* __restrict__ cursor,
+                                    int* __restrict__ out_col,
+                                    float* __restrict__ out_val) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < nnz;
+       e += gridDim.x * blockDim.x) {
+    // column of entry e: last k with colptr[k] <= e
+    int lo = 0, hi = kdim;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(colptr + mid) <= e) lo = mid; else hi = mid - 1;
+    }
+    const int r = rowidx[e];
+    if ((unsigned)r >= (unsigned)m) continue;
+    const int pos = atomicAdd(cursor + r, 1);
+    out_col[pos] = lo;
+    out_val[pos] = val[e];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row analysis + symbolic binning
+// ---------------------------------------------------------------------------
+
+constexpr int RA_THREADS = 256;
+constexpr int RA_ROWS = 64;  // rows per block
+
+// Per row i: P_i = sum over A(i,k) of nnz(B(k,:)) (the intermediate product
+// count the reference accumulates per row in initGEMM, src/mm.cu:138-148),
+// the flattened offset of each A entry, and the symbolic bin. Rows are
+// appended to their bin's list with one global atomic per bin per block.
+__global__ void __launch_bounds__(RA_THREADS)
+k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_p,
+               int* __restrict__ c_cnt, int* __restrict__ sym_count,
+               int* __restrict__ sym_rows, unsigned long long* __restrict__ p_total,
+               unsigned* status, Tuning tn) {
+  __shared__ int hist[SB_COUNT], base[SB_COUNT];
+  __shared__ int rowbin[RA_ROWS], rowrank[RA_ROWS];
+  __shared__ unsigned long long block_p;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = blockIdx.x * RA_ROWS;
+  if (threadIdx.x < SB_COUNT) hist[threadIdx.x] = 0;
+  if (threadIdx.x == 0) block_p = 0;
+  __syncthreads();
+  for (int lr = warp; lr < RA_ROWS; lr += RA_THREADS / 32) {
+    const int i = row0 + lr;
+    if (i >= op.m) {
+      if (lane == 0) rowbin[lr] = -1;
+      continue;
+    }
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    long long acc = 0;
+    for (int b = rs; b < re; b += 32) {
+      const int j = b + lane;
+      long long len = 0;
+      if (j < re) {
+        const int k = op.a_col[j];
+        if ((unsigned)k < (unsigned)op.kdim) len = op.b_rowptr[k + 1] - op.b_rowptr[k];
+        else atomicOr(status, ST_BAD_INDEX);
+      }
+      const long long incl = warp_incl_scan64(len);
+      if (j < re) aoff[j] = (int)(acc + incl - len);
+      acc += __shfl_sync(FULL, incl, 31);
+    }
+    if (lane == 0) {
+      row_p[i] = acc;
+      if (acc >= (1ll << 31)) atomicOr(status, ST_ROW_TOO_LONG);
+      const int bin = sym_bin_of(acc, op.n, tn);
+      if (bin < 0) c_cnt[i] = 0;
+      rowbin[lr] = bin;
+      if (bin >= 0) rowrank[lr] = atomicAdd(&hist[bin], 1);
+      atomicAdd(&block_p, (unsigned long long)acc);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < SB_COUNT && hist[threadIdx.x])
+    base[threadIdx.x] = atomicAdd(sym_count + threadIdx.x, hist[threadIdx.x]);
+  if (threadIdx.x == 0) atomicAdd(p_total, block_p);
+  __syncthreads();
+  for (int lr = threadIdx.x; lr < RA_ROWS; lr += RA_THREADS) {
+    const int b = rowbin[lr];
+    if (b >= 0) sym_rows[(size_t)b * op.m + base[b] + rowrank[lr]] = row0 + lr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Symbolic pass
+// ---------------------------------------------------------------------------
+
+constexpr int SW_THREADS = 256;  // warp-per-row kernels: 8 warps per block
+
+template <int LOG2T>
+__global__ void __launch_bounds__(SW_THREADS)
+k_sym_warp(Operands op, const int* __restrict__ rows, int nrows, int* __restrict__ c_cnt,
+           unsigned* status) {
+  constexpr int T = 1 << LOG2T;
+  constexpr int WPB = SW_THREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned* keys = reinterpret_cast<unsigned*>(smem) + warp * T;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * 4) + warp;
+  for (int r = blockIdx.x * WPB + warp; r < nrows; r += gridDim.x * WPB) {
+    const int i = rows[r];
+    for (int t = lane; t < T; t += 32) keys[t] = EMPTY_KEY;
+    __syncwarp();
+    SymHash f{keys, LOG2T, status, 0};
+    warp_expand_row<false>(op, op.a_rowptr[i], op.a_rowptr[i + 1], f, sc);
+    const int u = warp_sum(f.nnew);
+    if (lane == 0) c_cnt[i] = u;
+    __syncwarp();
+  }
+}
+
+constexpr int BLOCK_CHUNK = 256;  // products per warp work unit in block-per-row kernels
+
+template <int LOG2T, int NT>
+__global__ void __launch_bounds__(NT)
+k_sym_block(Operands op, const int* __restrict__ rows, int nrows,
+            const long long* __restrict__ row_p, int* __restrict__ c_cnt,
+            unsigned* status) {
+  constexpr int T = 1 << LOG2T;
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int total;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned* keys = reinterpret_cast<unsigned*>(smem);
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * 4) + warp;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int i = rows[r];
+    const int p = (int)row_p[i];
+    for (int t = threadIdx.x; t < T; t += NT) keys[t] = EMPTY_KEY;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    SymHash f{keys, LOG2T, status, 0};
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
+      warp_expand_range<false>(op, rs, re, c0, min(c0 + BLOCK_CHUNK, p), f, sc);
+    const int u = warp_sum(f.nnew);
+    if (lane == 0 && u) atomicAdd(&total, u);
+    __syncthreads();
+    if (threadIdx.x == 0) c_cnt[i] = total;
+    __syncthreads();
+  }
+}
+
+constexpr int LONG_THREADS = 1024;
+constexpr int LONG_CHUNK = 1024;  // products per warp work unit in long-row kernels
+
+// Exact nnz of long rows: presence bitmap of the row's columns in shared
+// memory, one window of `tn.sym_window` columns at a time. Also records the
+// nnz of every 2048-column chunk, from which k_num_bin cuts column slices.
+__global__ void __launch_bounds__(LONG_THREADS)
+k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
+           const long long* __restrict__ row_p, int* __restrict__ c_cnt,
+           int* __restrict__ long_slot, int* __restrict__ chunk_cnt, int n_chunks,
+           unsigned* status, Tuning tn) {
+  constexpr int NW = LONG_THREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int total;
+  __shared__ int next_batch;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
+  unsigned* bits = reinterpret_cast<unsigned*>(smem + NW * sizeof(SegScratch));
+  const int n = op.n;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int i = rows[r];
+    const int p = (int)row_p[i];
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    if (threadIdx.x == 0) { total = 0; long_slot[i] = r; }
+    for (int w0 = 0; w0 < n; w0 += tn.sym_window) {
+      const int wcols = min(n - w0, tn.sym_window);
+      const int nw = (wcols + 31) >> 5;
+      for (int t = threadIdx.x; t < nw; t += LONG_THREADS) bits[t] = 0u;
+      if (threadIdx.x == 0) next_batch = 0;
+      __syncthreads();
+      SymBits f{bits, w0, (unsigned)wcols, status};
+      if (w0 == 0 && wcols == n) {
+        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
+          warp_expand_range<false>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
+      } else {
+        for (;;) {
+          int jb = 0;
+          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
+          jb = __shfl_sync(FULL, jb, 0);
+          if (jb >= re) break;
+          warp_expand_restricted<false>(op, jb, re, w0, w0 + wcols, f, sc);
+        }
+      }
+      __syncthreads();
+      // chunk counts (w0 is a multiple of CHUNK_COLS)
+      const int nchunk_w = (nw + CHUNK_WORDS - 1) / CHUNK_WORDS;
+      for (int c = warp; c < nchunk_w; c += NW) {
+        int v = 0;
+        for (int t = lane; t < CHUNK_WORDS; t += 32) {
+          const int w = c * CHUNK_WORDS + t;
+          if (w < nw) v += __popc(bits[w]);
+        }
+        v = warp_sum(v);
+        if (lane == 0) {
+          chunk_cnt[(size_t)r * n_chunks + w0 / CHUNK_COLS + c] = v;
+          if (v) atomicAdd(&total, v);
+        }
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) c_cnt[i] = total;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Scan (row pointers of C)
+// ---------------------------------------------------------------------------
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ long long block_excl_scan64(long long v, long long* shm,
+                                                       long long& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long long incl = warp_incl_scan64(v);
+  if (lane == 31) shm[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const long long w = (lane < (int)(blockDim.x >> 5)) ? shm[lane] : 0;
+    const long long wi = warp_incl_scan64(w);
+    shm[lane] = wi - w;
+    if (lane == 31) shm[32] = wi;
+  }
+  __syncthreads();
+  const long long r = shm[warp] + incl - v;
+  total = shm[32];
+  __syncthreads();
+  return r;
+}
+
+// Phase 1: per-tile sums of an int32 array.
+__global__ void __launch_bounds__(SCAN_THREADS)
+k_scan_tiles(const int* __restrict__ in, int n, long long* __restrict__ tile_sum) {
+  __shared__ long long shm[33];
+  const long long base = (long long)blockIdx.x * SCAN_TILE;
+  long long v = 0;
+#pragma unroll
+  for (int q = 0; q < SCAN_ITEMS; ++q) {
+    const long long idx = base + threadIdx.x * SCAN_ITEMS + q;
+    if (idx < n) v += in[idx];
+  }
+  long long total;
+  block_excl_scan64(v, shm, total);
+  if (threadIdx.x == 0) tile_sum[blockIdx.x] = total;
+}
+
+// Phase 2: exclusive scan of the tile sums (single block, looping).
+__global__ void __launch_bounds__(SCAN_THREADS)
+k_scan_tile_sums(long long* __restrict__ tile_sum, int ntiles,
+                 long long* __restrict__ grand_total) {
+  __shared__ long long shm[33];
+  long long carry = 0;
+  for (int b = 0; b < ntiles; b += SCAN_THREADS) {
+    const int idx = b + threadIdx.x;
+    const long long v = idx < ntiles ? tile_sum[idx] : 0;
+    long long total;
+    const long long ex = block_excl_scan64(v, shm, total);
+    if (idx < ntiles) tile_sum[idx] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) *grand_total = carry;
+}
+
+// Phase 3: out[i] = exclusive prefix of in (int64), out[n] = total.
+__global__ void __launch_bounds__(SCAN_THREADS)
+k_scan_apply(const int* __restrict__ in, int n, const long long* __restrict__ tile_off,
+             const long long* __restrict__ grand_total, long long* __restrict__ out) {
+  __shared__ long long shm[33];
+  const long long base = (long long)blockIdx.x * SCAN_TILE;
+  int v[SCAN_ITEMS];
+  long long sum = 0;
+#pragma unroll
+  for (int q = 0; q < SCAN_ITEMS; ++q) {
+    const long long idx = base + threadIdx.x * SCAN_ITEMS + q;
+    v[q] = idx < n ? in[idx] : 0;
+    sum += v[q];
+  }
+  long long total;
+  long long run = block_excl_scan64(sum, shm, total) + tile_off[blockIdx.x];
+#pragma unroll
+  for (int q = 0; q < SCAN_ITEMS; ++q) {
+    const long long idx = base + threadIdx.x * SCAN_ITEMS + q;
+    if (idx < n) out[idx] = run;
+    run += v[q];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = *grand_total;
+}
+
+// int64 row pointers -> the int32 row pointers of the cm boundary.
+__global__ void k_rowptr_to_i32(const long long* __restrict__ in, int n1,
+                                int* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += gridDim.x * blockDim.x)
+    out[i] = (int)in[i];
+}
+
+// int32 CSC/CSR pointer array from counts (used by the transpose).
+__global__ void k_rowptr_i64_to_i32_shift(const long long* __restrict__ in, int n1,
+                                          int* __restrict__ out, int* __restrict__ out2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += gridDim.x * blockDim.x) {
+    out[i] = (int)in[i];
+    if (out2) out2[i] = (int)in[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Numeric binning + long-row slicing
+// ---------------------------------------------------------------------------
+
+constexpr int NBIN_THREADS = 256;
+
+__global__ void __launch_bounds__(NBIN_THREADS)
+k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restrict__ row_p,
+          const long long* __restrict__ c_rowptr, int* __restrict__ num_count,
+          int* __restrict__ num_rows, const int* __restrict__ long_slot,
+          const int* __restrict__ chunk_cnt, int n_chunks, Slice* __restrict__ slices,
+          int* __restrict__ slice_count, int slice_capacity, unsigned* status, Tuning tn) {
+  __shared__ int hist[NB_COUNT], base[NB_COUNT];
+  const int i = blockIdx.x * NBIN_THREADS + threadIdx.x;
+  if (threadIdx.x < NB_COUNT) hist[threadIdx.x] = 0;
+  __syncthreads();
+  int bin = -1, rank = 0;
+  if (i < m) {
+    const int o = c_cnt[i];
+    bin = num_bin_of(o, row_p[i], tn);
+    if (bin == NB_LONG) {
+      const long long out0 = c_rowptr[i];
+      if (o <= tn.slice_cap && n <= tn.slice_cols) {
+        const int s = atomicAdd(slice_count, 1);
+        if (s < slice_capacity) slices[s] = Slice{out0, i, 0, n, o};
+        else atomicOr(status, ST_SLICE_OVERFLOW);
+      } else {
+        const int* cc = chunk_cnt + (size_t)long_slot[i] * n_chunks;
+        int lo_c = 0, acc = 0;
+        long long out = out0;
+        for (int c = 0; c < n_chunks; ++c) {
+          const int v = cc[c];
+          const bool too_many = acc + v > tn.slice_cap;
+          const bool too_wide = (c + 1 - lo_c) * CHUNK_COLS > tn.slice_cols;
+          if ((too_many || too_wide) && c > lo_c) {
+            if (acc) {
+              const int s = atomicAdd(slice_count, 1);
+              if (s < slice_capacity) slices[s] = Slice{out, i, lo_c * CHUNK_COLS, c * CHUNK_COLS, acc};
+              else atomicOr(status, ST_SLICE_OVERFLOW);
+            }
+            out += acc;
+            lo_c = c;
+            acc = 0;
+          }
+          acc += v;
+        }
+        if (acc) {
+          const int s = atomicAdd(slice_count, 1);
+          if (s < slice_capacity) slices[s] = Slice{out, i, lo_c * CHUNK_COLS, n, acc};
+          else atomicOr(status, ST_SLICE_OVERFLOW);
+        }
+      }
+      bin = -1;
+    } else if (bin >= 0) {
+      rank = atomicAdd(&hist[bin], 1);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < NB_COUNT && hist[threadIdx.x])
+    base[threadIdx.x] = atomicAdd(num_count + threadIdx.x, hist[threadIdx.x]);
+  __syncthreads();
+  if (bin >= 0) num_rows[(size_t)bin * m + base[bin] + rank] = i;
+}
+
+// ---------------------------------------------------------------------------
+// Numeric pass: hash rows
+// ---------------------------------------------------------------------------
+
+// Value slot type of each precision mode (0 plain, 1 compensated).
+template <int MODE> struct SlotOf { using T = float; };
+template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or double bits
+
+template <int LOG2T, int MODE>
+__global__ void __launch_bounds__(SW_THREADS)
+k_num_warp(Operands op, const int* __restrict__ rows, int nrows,
+           const long long* __restrict__ c_rowptr, int* __restrict__ c_col,
+           float* __restrict__ c_val, unsigned* status) {
+  constexpr int T = 1 << LOG2T;
+  constexpr int WPB = SW_THREADS / 32;
+  using V = typename SlotOf<MODE>::T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  V* vals = reinterpret_cast<V*>(smem) + warp * T;
+  unsigned* keys = reinterpret_cast<unsigned*>(smem + WPB * T * sizeof(V)) + warp * T;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * (sizeof(V) + 4)) + warp;
+  for (int r = blockIdx.x * WPB + warp; r < nrows; r += gridDim.x * WPB) {
+    const int i = rows[r];
+    for (int t = lane; t < T; t += 32) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
+    __syncwarp();
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    if (MODE == 0) {
+      NumHashPlain f{keys, reinterpret_cast<float*>(vals), LOG2T, status};
+      warp_expand_row<true>(op, rs, re, f, sc);
+    } else {
+      // warp rows have P_i <= warp_p_max_num <= 4096: TwoSum, no FP64
+      NumHashTwoSum f{keys, reinterpret_cast<float2*>(vals), LOG2T, status};
+      warp_expand_row<true>(op, rs, re, f, sc);
+    }
+    __syncwarp();
+    bitonic_sort_kv<T, 32>(keys, vals, lane, WarpSync());
+    const long long o = c_rowptr[i];
+    const int cnt = (int)(c_rowptr[i + 1] - o);
+    if (lane == 0 && ((cnt < T && keys[cnt] != EMPTY_KEY) || keys[cnt - 1] == EMPTY_KEY))
+      atomicOr(status, ST_COUNT_MISMATCH);
+    for (int t = lane; t < cnt; t += 32) {
+      c_col[o + t] = (int)keys[t];
+      if (MODE == 0) c_val[o + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+      else c_val[o + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    }
+    __syncwarp();
+  }
+}
+
+template <int LOG2T, int NT, int MODE>
+__global__ void __launch_bounds__(NT)
+k_num_block(Operands op, const int* __restrict__ rows, int nrows,
+            const long long* __restrict__ row_p, const long long* __restrict__ c_rowptr,
+            int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
+  constexpr int T = 1 << LOG2T;
+  constexpr int NW = NT / 32;
+  using V = typename SlotOf<MODE>::T;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int warp = threadIdx.x >> 5;
+  V* vals = reinterpret_cast<V*>(smem);
+  unsigned* keys = reinterpret_cast<unsigned*>(smem + T * sizeof(V));
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * (sizeof(V) + 4)) + warp;
+  for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    const int i = rows[r];
+    const long long p = row_p[i];
+    for (int t = threadIdx.x; t < T; t += NT) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
+    __syncthreads();
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    const bool fp64 = MODE == 1 && p > FP64_ROW_PARTIALS;
+    if (MODE == 0) {
+      NumHashPlain f{keys, reinterpret_cast<float*>(vals), LOG2T, status};
+      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+    } else if (fp64) {
+      NumHashF64 f{keys, reinterpret_cast<double*>(vals), LOG2T, status};
+      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+    } else {
+      NumHashTwoSum f{keys, reinterpret_cast<float2*>(vals), LOG2T, status};
+      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+    }
+    __syncthreads();
+    bitonic_sort_kv<T, NT>(keys, vals, threadIdx.x, BlockSync());
+    const long long o = c_rowptr[i];
+    const int cnt = (int)(c_rowptr[i + 1] - o);
+    if (threadIdx.x == 0 &&
+        ((cnt < T && keys[cnt] != EMPTY_KEY) || keys[cnt - 1] == EMPTY_KEY))
+      atomicOr(status, ST_COUNT_MISMATCH);
+    for (int t = threadIdx.x; t < cnt; t += NT) {
+      c_col[o + t] = (int)keys[t];
+      if (MODE == 0) c_val[o + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+      else if (fp64) c_val[o + t] = finalize_value(reinterpret_cast<double*>(vals)[t]);
+      else c_val[o + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Numeric pass: long rows, one block per column slice
+// ---------------------------------------------------------------------------
+
+// Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap].
+// Pass 1 sets presence bits, a block scan turns popcounts into ranks, pass 2
+// adds every product into the slot given by its column's rank, and the slice
+// is written out in column order straight from the bitmap.
+template <int MODE>
+__global__ void __launch_bounds__(LONG_THREADS)
+k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
+           const long long* __restrict__ row_p, int dir_words, int cap,
+           int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
+  constexpr int NW = LONG_THREADS / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long scan_shm[33];
+  __shared__ int next_batch;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
+  uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
+  unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
+  for (int s = blockIdx.x; s < nslices; s += gridDim.x) {
+    const Slice sl = slices[s];
+    const int i = sl.row;
+    const int p = (int)row_p[i];
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    const bool full = sl.lo == 0 && sl.hi == op.n;
+    const int nw = (sl.hi - sl.lo + 31) >> 5;
+    const int cnt = sl.cnt;
+    if (nw > dir_words || cnt > cap) {  // host sizing guarantees this never trips
+      if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
+      continue;
+    }
+    for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(0u, 0u);
+    if (threadIdx.x == 0) next_batch = 0;
+    __syncthreads();
+    // pass 1: presence bits
+    {
+      LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
+      if (full) {
+        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
+          warp_expand_range<false>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
+      } else {
+        for (;;) {
+          int jb = 0;
+          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
+          jb = __shfl_sync(FULL, jb, 0);
+          if (jb >= re) break;
+          warp_expand_restricted<false>(op, jb, re, sl.lo, sl.hi, f, sc);
+        }
+      }
+    }
+    __syncthreads();
+    // ranks: exclusive scan of popcounts over the nw directory words
+    long long tot;
+    {
+      const int per = (nw + LONG_THREADS - 1) / LONG_THREADS;
+      const int w0 = threadIdx.x * per;
+      int local = 0;
+      for (int q = 0; q < per; ++q)
+        if (w0 + q < nw) local += __popc(dir[w0 + q].x);
+      long long run = block_excl_scan64(local, scan_shm, tot);
+      for (int q = 0; q < per; ++q)
+        if (w0 + q < nw) { dir[w0 + q].y = (unsigned)run; run += __popc(dir[w0 + q].x); }
+      if (threadIdx.x == 0) next_batch = 0;
+    }
+    if (tot != cnt) {  // block-uniform: slots would not fit the slice
+      if (threadIdx.x == 0) atomicOr(status, ST_COUNT_MISMATCH);
+      __syncthreads();
+      continue;
+    }
+    if (MODE == 0) {
+      float* vals = reinterpret_cast<float*>(vbase);
+      for (int t = threadIdx.x; t < cnt; t += LONG_THREADS) vals[t] = 0.f;
+    } else {
+      double* vals = reinterpret_cast<double*>(vbase);
+      for (int t = threadIdx.x; t < cnt; t += LONG_THREADS) vals[t] = 0.0;
+    }
+    __syncthreads();
+    // pass 2: values
+    if (MODE == 0) {
+      LongValPlain f{dir, reinterpret_cast<float*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      if (full) {
+        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
+          warp_expand_range<true>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
+      } else {
+        for (;;) {
+          int jb = 0;
+          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
+          jb = __shfl_sync(FULL, jb, 0);
+          if (jb >= re) break;
+          warp_expand_restricted<true>(op, jb, re, sl.lo, sl.hi, f, sc);
+        }
+      }
+    } else {
+      LongValF64 f{dir, reinterpret_cast<double*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      if (full) {
+        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
+          warp_expand_range<true>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
+      } else {
+        for (;;) {
+          int jb = 0;
+          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
+          jb = __shfl_sync(FULL, jb, 0);
+          if (jb >= re) break;
+          warp_expand_restricted<true>(op, jb, re, sl.lo, sl.hi, f, sc);
+        }
+      }
+    }
+    __syncthreads();
+    // write out in column order
+    for (int w = threadIdx.x; w < nw; w += LONG_THREADS) {
+      unsigned bitsw = dir[w].x;
+      int rnk = (int)dir[w].y;
+      while (bitsw) {
+        const int b = __ffs(bitsw) - 1;
+        bitsw &= bitsw - 1u;
+        const long long o = sl.out + rnk;
+        c_col[o] = sl.lo + w * 32 + b;
+        if (MODE == 0) c_val[o] = reinterpret_cast<float*>(vbase)[rnk];
+        else c_val[o] = finalize_value(reinterpret_cast<double*>(vbase)[rnk]);
+        ++rnk;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace sg

@@ -1,0 +1,151 @@
+"""GPU parity: the sm_100a engine (through the C ABI) against the FP64 oracle.
+
+Structure (row pointers, sorted column indices, explicit zeros) must be
+bit-exact; values must lie within the summation-error bounds stated in
+helpers.py (plain FP32 and compensated modes)."""
+import numpy as np
+import pytest
+
+import oracle
+import spgemm_b200 as sg
+from spgemm_b200 import workloads as W
+from helpers import (assert_structure_equal, assert_values_close, compensated_tolerance,
+                     plain_tolerance, rel_error_report)
+
+pytestmark = pytest.mark.gpu
+
+
+def ref_product(A, B, rows=None):
+    a = A.to_csc()
+    return oracle.spgemm(A.rows, B.cols, a.colptr, a.rowidx, a.val, B.rowptr, B.col, B.val,
+                         rows=rows, stats=True)
+
+
+def check(A, B, precision=sg.PLAIN, a_format="csc", ref=None):
+    Aop = A.to_csc() if a_format == "csc" else A
+    with sg.Handle(precision) as h:
+        C = h.multiply_host(Aop, B)
+        stats = h.stats()
+    ref = ref_product(A, B) if ref is None else ref
+    assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+    tol = plain_tolerance(ref) if precision == sg.PLAIN else compensated_tolerance(ref)
+    assert_values_close(C.val, ref, tol)
+    assert stats["intermediate_products"] == ref["products"]
+    assert stats["nnz_c"] == len(ref["col"])
+    return C, ref, stats
+
+
+def dense_csr(D):
+    D = np.asarray(D, np.float32)
+    r, c = np.nonzero(D)
+    return W.from_coo(D.shape[0], D.shape[1], r, c, D[r, c])
+
+
+def test_er4096_plain():
+    A = W.er(4096, 8.0, 0)
+    _, ref, stats = check(A, A)
+    assert stats["kernel_launches"] > 0
+
+
+def test_er4096_compensated():
+    A = W.er(4096, 8.0, 0)
+    check(A, A, sg.COMPENSATED)
+
+
+def test_a_as_csr_equals_csc():
+    A = W.er(2000, 10.0, 3)
+    check(A, A, a_format="csr")
+
+
+def test_kat_cancellation_and_empty_rows():
+    A = W.from_coo(3, 2, np.array([0, 0, 2]), np.array([0, 1, 1]), np.array([1, 1, 4], np.float32))
+    B = W.from_coo(2, 2, np.array([0, 0, 1]), np.array([0, 1, 0]), np.array([2, 3, -2], np.float32))
+    C, _, _ = check(A, B)
+    assert C.rowptr.tolist() == [0, 2, 2, 3]
+    assert C.col.tolist() == [0, 1, 0]
+    assert C.val.tolist() == [0.0, 3.0, -8.0]
+
+
+def test_rectangular_and_empty_columns():
+    rng = np.random.default_rng(7)
+    D1 = (rng.random((37, 53)) < 0.1) * rng.uniform(-1, 1, (37, 53))
+    D2 = (rng.random((53, 91)) < 0.1) * rng.uniform(-1, 1, (53, 91))
+    D1[:, 5] = 0
+    D2[10, :] = 0
+    check(dense_csr(D1), dense_csr(D2))
+
+
+def test_empty_product():
+    A = W.Csr(5, 4, np.zeros(6, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
+    B = dense_csr(np.eye(4))
+    C, _, _ = check(A, B)
+    assert C.nnz == 0 and C.rowptr.tolist() == [0] * 6
+
+
+def test_rmat_all_bins():
+    A = W.rmat(13, 16, 1)
+    _, _, stats = check(A, A)
+    assert stats["rows_per_symbolic_bin"][8] > 0, stats
+    assert stats["rows_per_numeric_bin"][8] > 0, stats
+
+
+def test_rmat_all_bins_compensated():
+    A = W.rmat(13, 16, 2)
+    check(A, A, sg.COMPENSATED)
+
+
+def test_long_rows_multi_slice_multi_window():
+    # one C row with ~1e5 outputs over 1.2M columns: several numeric slices
+    # and two symbolic bitmap windows
+    rng = np.random.default_rng(11)
+    n = 1_200_000
+    kk = 220
+    rows, cols = [], []
+    for k in range(kk):
+        c = np.unique(rng.integers(0, n, 600))
+        rows.append(np.full(len(c), k))
+        cols.append(c)
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    B = W.from_coo(kk, n, r, c, rng.uniform(-1, 1, len(r)).astype(np.float32))
+    A = W.from_coo(3, kk, np.array([0] * kk + [2] * 50), np.concatenate([np.arange(kk), np.arange(50)]),
+                   rng.uniform(-1, 1, kk + 50).astype(np.float32))
+    _, _, stats = check(A, B)
+    assert stats["long_row_slices"] >= 3, stats
+    check(A, B, sg.COMPENSATED)
+
+
+def test_galerkin_chain_small():
+    A = W.stencil27(8, values="laplace")
+    P = W.prolongator(8)
+    with sg.Handle(sg.COMPENSATED) as h:
+        AP = h.multiply_host(A.to_csc(), P)
+        PtAP = h.multiply_host(P.transpose().to_csc(), AP)
+    ref_ap = ref_product(A, P)
+    assert_structure_equal(AP.rowptr, AP.col, ref_ap["rowptr"], ref_ap["col"])
+    assert_values_close(AP.val, ref_ap, compensated_tolerance(ref_ap))
+    ref = ref_product(P.transpose(), AP)
+    assert_structure_equal(PtAP.rowptr, PtAP.col, ref["rowptr"], ref["col"])
+    assert_values_close(PtAP.val, ref, compensated_tolerance(ref))
+
+
+@pytest.mark.parametrize("precision", [sg.PLAIN, sg.COMPENSATED])
+def test_stencil_small(precision):
+    A = W.stencil27(14, seed=3)
+    C, ref, _ = check(A, A, precision)
+    if precision == sg.COMPENSATED:
+        rep = rel_error_report(C.val, ref)
+        assert rep["max_rel"] < 1e-6 or rep["worst_cond"] > 1e7, rep
+
+
+def test_repeat_calls_reuse_workspace():
+    A = W.er(3000, 8.0, 9)
+    B = W.rmat(11, 8, 9)
+    with sg.Handle() as h:
+        for M in (A, W.er(1000, 4.0, 1), A):
+            C = h.multiply_host(M.to_csc(), M)
+            ref = ref_product(M, M)
+            assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+        C = h.multiply_host(B.to_csc(), B)
+        ref = ref_product(B, B)
+        assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
