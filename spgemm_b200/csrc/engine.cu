@@ -103,8 +103,8 @@ int Engine::prof_collect() {
 Engine::~Engine() {
   DevBuf* all[] = {&a_rowptr_, &a_col_, &a_val_, &cursor_, &aoff_, &row_p_, &c_cnt_,
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
-                   &chunk_cnt_, &slices_buf_, &counters_, &out_rowptr_, &out_col_,
-                   &out_val_};
+                   &chunk_cnt_, &slices_buf_, &counters_, &restrict_scratch_, &out_rowptr_,
+                   &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
   for (DevBuf& b : stage_) b.release();
   if (host_counters_) cudaFreeHost(host_counters_);
@@ -306,7 +306,7 @@ int Engine::analyze(const cm& A, const cm& B) {
     prof_begin("k_row_analysis");
     k_row_analysis<<<(m + RA_ROWS - 1) / RA_ROWS, RA_THREADS, 0, stream_>>>(
         op_, aoff_.as<int>(), row_p_.as<long long>(), c_cnt_.as<int>(), dc->sym_count,
-        sym_rows_.as<int>(), &dc->p_total, &dc->status, tn_);
+        sym_rows_.as<int>(), &dc->p_total, &dc->max_row_len, &dc->status, tn_);
     SG_LAUNCHED("k_row_analysis");
   }
   SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
@@ -316,6 +316,7 @@ int Engine::analyze(const cm& A, const cm& B) {
   p_total_ = (long long)host_counters_->p_total;
   for (int b = 0; b < SB_COUNT; ++b) sym_counts_[b] = host_counters_->sym_count[b];
   n_long_sym_ = sym_counts_[SB_LONG];
+  max_row_len_ = host_counters_->max_row_len;
   n_chunks_ = (n_ + CHUNK_COLS - 1) / CHUNK_COLS;
   have_analysis_ = true;
   return 0;
@@ -389,10 +390,16 @@ int Engine::launch_symbolic_bins() {
     const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)((win + 31) / 32) * 4;
     SG_CK(smem_attr(k_sym_long, smem), "smem attr k_sym_long");
     const int cnt = sym_counts_[SB_LONG];
+    const int grid = blocks_for(cnt, 1, (long long)sms_ * 2);
+    const int stride = 2 * max_row_len_ + 2;
+    if (n_ > tn_.sym_window)
+      SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
+    else
+      SG_CK(restrict_scratch_.ensure(16), "alloc restrict scratch");
     prof_begin("k_sym_long");
-    k_sym_long<<<blocks_for(cnt, 1, (long long)sms_ * 2), LONG_THREADS, smem, stream_>>>(
+    k_sym_long<<<grid, LONG_THREADS, smem, stream_>>>(
         op, rows + (size_t)SB_LONG * m, cnt, row_p, c_cnt, long_slot_.as<int>(),
-        chunk_cnt_.as<int>(), n_chunks_, status, tn_);
+        chunk_cnt_.as<int>(), n_chunks_, restrict_scratch_.as<int>(), stride, status, tn_);
     SG_LAUNCHED("k_sym_long");
   }
 #define SG_SYM_WARP(L)                                                                    \
@@ -432,7 +439,8 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
                                const int* nslices_dev, const long long* row_p,
                                const long long* c_rowptr, int* c_col, float* c_val,
                                unsigned* status, cudaStream_t stream, int sms, int n,
-                               int slice_cols, int slice_cap, long long& launches);
+                               int slice_cols, int slice_cap, DevBuf& scratch,
+                               int max_row_len, long long& launches);
 
 int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
@@ -458,12 +466,12 @@ int Engine::launch_numeric_bins(int* c_col, float* c_val) {
                                   slices_buf_.as<Slice>(), &dc->slice_count,
                                   row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
                                   c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                  tn_run_slice_cap_, launches_);
+                                  tn_run_slice_cap_, restrict_scratch_, max_row_len_, launches_);
   return launch_numeric_impl<1>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
                                 slices_buf_.as<Slice>(), &dc->slice_count,
                                 row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
                                 c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                tn_run_slice_cap_, launches_);
+                                tn_run_slice_cap_, restrict_scratch_, max_row_len_, launches_);
 }
 
 template <class K>
@@ -490,7 +498,8 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
                                const int* nslices_dev, const long long* row_p,
                                const long long* c_rowptr, int* c_col, float* c_val,
                                unsigned* status, cudaStream_t stream, int sms, int n,
-                               int slice_cols, int slice_cap, long long& launches) {
+                               int slice_cols, int slice_cap, DevBuf& scratch,
+                               int max_row_len, long long& launches) {
   constexpr int WPB = SW_THREADS / 32;
   constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
   if (nslices > 0) {
@@ -499,9 +508,13 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
     const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES +
                         (size_t)dir_words * sizeof(uint2) + (size_t)slice_cap * (MODE ? 8 : 4);
     SG_CKE(set_smem(k_num_long<MODE>, smem), "smem attr k_num_long");
+    const int grid = blocks_for(nslices, 1, (long long)sms * 2);
+    const int stride = 2 * max_row_len + 2;
+    SG_CKE(scratch.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
     E.prof_begin("k_num_long");
-    k_num_long<MODE><<<blocks_for(nslices, 1, (long long)sms * 2), LONG_THREADS, smem, stream>>>(
-        op, slices, nslices, row_p, dir_words, slice_cap, c_col, c_val, status);
+    k_num_long<MODE><<<grid, LONG_THREADS, smem, stream>>>(
+        op, slices, nslices, row_p, dir_words, slice_cap, scratch.as<int>(), stride, c_col,
+        c_val, status);
     SG_LAUNCHED_E("k_num_long");
   }
 #define SG_NUM_WARP(L)                                                                       \

@@ -32,6 +32,7 @@ struct DevCounters {
   unsigned status;
   unsigned long long p_total;
   long long grand_total;
+  int max_row_len;  // longest row of A (entries)
 };
 
 class Engine {
@@ -123,7 +124,8 @@ class Engine {
   DevBuf a_rowptr_, a_col_, a_val_, cursor_, aoff_;
   DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
   DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_;
-  DevBuf counters_;
+  DevBuf counters_, restrict_scratch_;
+  int max_row_len_ = 0;
   DevBuf out_rowptr_, out_col_, out_val_;
   DevBuf stage_[6];
   DevCounters* host_counters_ = nullptr;  // pinned

@@ -131,33 +131,68 @@ __device__ __forceinline__ int compact_segments(int& bstart, int& len, float& a,
 // time, so lanes stay busy whatever the segment lengths. The owner of each
 // product is found from the OR of segment-start bits in the current window
 // (redux.sync) and a popcount -- O(1) per product, no search.
+//
+// Each segment is walked from a pseudo-random starting offset (wrapping
+// around). B's rows are sorted, so without the rotation every warp would
+// begin its segments on the same lowest (for power-law graphs: the most
+// popular) columns at the same time, and the shared-memory atomics of all
+// warps would collide there.
 template <bool NEED_VAL, class F>
 __device__ __forceinline__ void run_segments(int cnt, int bstart, int len, float a,
                                              const int* __restrict__ b_col,
                                              const float* __restrict__ b_val, F& f) {
+  constexpr int UNROLL = 4;  // windows whose loads are issued before their accumulates
   const int lane = lane_id();
   if (lane >= cnt) len = 0;
   const int incl = warp_incl_scan(len);
   const int total = __shfl_sync(FULL, incl, 31);
   const int s = incl - len;
+  const int rot = len > 1 ? (int)(((unsigned)bstart * 2654435761u >> 8) % (unsigned)len) : 0;
   int nbefore = 0;
-  for (int base = 0; base < total; base += 32) {
-    const unsigned bit =
-        (len > 0 && s >= base && s < base + 32) ? (1u << (s - base)) : 0u;
-    const unsigned starts = __reduce_or_sync(FULL, bit);
-    const int owner = nbefore + __popc(starts & (FULL >> (31 - lane))) - 1;
-    nbefore += __popc(starts);
-    const int ob = __shfl_sync(FULL, bstart, owner);
-    const int os = __shfl_sync(FULL, s, owner);
-    const float oa = __shfl_sync(FULL, a, owner);
-    const int fp = base + lane;
-    if (fp < total) {
-      const int pos = ob + (fp - os);
-      const int col = __ldg(b_col + pos);
-      const float bv = NEED_VAL ? __ldg(b_val + pos) : 0.f;
-      f(col, oa, bv);
+  for (int base = 0; base < total; base += 32 * UNROLL) {
+    int col[UNROLL];
+    float bv[UNROLL], oa[UNROLL];
+    bool ok[UNROLL];
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u) {
+      const int wb = base + 32 * u;
+      ok[u] = false;
+      if (wb < total) {  // warp-uniform
+        const unsigned bit =
+            (len > 0 && s >= wb && s < wb + 32) ? (1u << (s - wb)) : 0u;
+        const unsigned starts = __reduce_or_sync(FULL, bit);
+        const int owner = nbefore + __popc(starts & (FULL >> (31 - lane))) - 1;
+        nbefore += __popc(starts);
+        const int ob = __shfl_sync(FULL, bstart, owner);
+        const int os = __shfl_sync(FULL, s, owner);
+        const int ol = __shfl_sync(FULL, len, owner);
+        const int orot = __shfl_sync(FULL, rot, owner);
+        oa[u] = __shfl_sync(FULL, a, owner);
+        const int fp = wb + lane;
+        if (fp < total) {
+          int off = fp - os + orot;
+          if (off >= ol) off -= ol;
+          const int pos = ob + off;
+          col[u] = __ldg(b_col + pos);
+          bv[u] = NEED_VAL ? __ldg(b_val + pos) : 0.f;
+          ok[u] = true;
+        }
+      }
     }
+#pragma unroll
+    for (int u = 0; u < UNROLL; ++u)
+      if (ok[u]) f(col[u], oa[u], bv[u]);
   }
+}
+
+// Products per warp work unit when the warps of a block share one row of
+// `p` products: about 8 units per warp, a multiple of 32, at least 64.
+__device__ __forceinline__ int chunk_for(long long p, int nwarps, int max_chunk) {
+  long long u = (p + nwarps * 8 - 1) / (nwarps * 8);
+  u = (u + 31) & ~31ll;
+  if (u < 64) u = 64;
+  if (u > max_chunk) u = max_chunk;
+  return (int)u;
 }
 
 // Whole row of A, one warp.
@@ -210,6 +245,97 @@ __device__ __forceinline__ void warp_expand_range(const Operands& op, int rs, in
         if (l1 > l0) {
           a = __ldg(op.a_val + j);
           bstart = bs + (l0 - off);
+          len = l1 - l0;
+        }
+      }
+    }
+    const bool done = __any_sync(FULL, past);
+    const int cnt = compact_segments(bstart, len, a, sc);
+    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+    if (done) break;
+  }
+}
+
+// Block-wide preparation of a column-restricted pass over one row: for each
+// entry j of the row (d = re - rs entries), the positions of B(k_j,:) whose
+// columns fall in [clo, chi) (binary search; B's rows are sorted) go to
+// seg_start[j] / roff (exclusive prefix of their lengths, roff[d] = total).
+// The arrays are this block's global scratch. Returns the total (block-uniform).
+__device__ __forceinline__ int block_restrict_row(const Operands& op, int rs, int re, int clo,
+                                                  int chi, int* seg_start, int* roff,
+                                                  long long* scan_shm, int* carry_shm) {
+  const int d = re - rs;
+  if (threadIdx.x == 0) *carry_shm = 0;
+  __syncthreads();
+  for (int t0 = 0; t0 < d; t0 += blockDim.x) {
+    const int t = t0 + threadIdx.x;
+    int s0 = 0, len = 0;
+    if (t < d) {
+      const int k = __ldg(op.a_col + rs + t);
+      const int bs = __ldg(op.b_rowptr + k), be = __ldg(op.b_rowptr + k + 1);
+      if (be > bs) {
+        const int first = __ldg(op.b_col + bs), last = __ldg(op.b_col + be - 1);
+        if (first < chi && last >= clo) {
+          s0 = first >= clo ? bs : lower_bound_i32(op.b_col, bs, be, clo);
+          const int s1 = last < chi ? be : lower_bound_i32(op.b_col, s0, be, chi);
+          len = s1 - s0;
+        }
+      }
+    }
+    // block exclusive scan of len (64-bit scan helper from the caller's shm)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int incl = warp_incl_scan(len);
+    if (lane == 31) scan_shm[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      const long long wv = lane < (int)(blockDim.x >> 5) ? scan_shm[lane] : 0;
+      const long long wi = warp_incl_scan64(wv);
+      scan_shm[lane] = wi - wv;
+      if (lane == 31) scan_shm[32] = wi;
+    }
+    __syncthreads();
+    const int carry = *carry_shm;
+    if (t < d) {
+      seg_start[t] = s0;
+      roff[t] = carry + (int)scan_shm[warp] + incl - len;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *carry_shm = carry + (int)scan_shm[32];
+    __syncthreads();
+  }
+  const int total = *carry_shm;
+  if (threadIdx.x == 0) roff[d] = total;
+  __syncthreads();
+  return total;
+}
+
+// Products [f0, f1) of a row prepared by block_restrict_row, one warp.
+// seg_start / roff are written by this block in this kernel, so they are read
+// with plain (coherent) loads.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_expand_explicit(const Operands& op, int rs, int d,
+                                                     const int* seg_start, const int* roff,
+                                                     int f0, int f1, F& f, SegScratch* sc) {
+  const int lane = lane_id();
+  int lo = 0, hi = d;  // last entry whose offset is <= f0
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (roff[mid] <= f0) lo = mid + 1; else hi = mid;
+  }
+  for (int base = lo - 1; base < d; base += 32) {
+    const int j = base + lane;
+    int bstart = 0, len = 0;
+    float a = 0.f;
+    bool past = true;
+    if (j < d) {
+      const int off = roff[j];
+      past = off >= f1;
+      if (!past) {
+        const int bl = roff[j + 1] - off;
+        const int l0 = max(off, f0), l1 = min(off + bl, f1);
+        if (l1 > l0) {
+          a = __ldg(op.a_val + rs + j);
+          bstart = seg_start[j] + (l0 - off);
           len = l1 - l0;
         }
       }

@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(RA_THREADS)
 k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_p,
                int* __restrict__ c_cnt, int* __restrict__ sym_count,
                int* __restrict__ sym_rows, unsigned long long* __restrict__ p_total,
-               unsigned* status, Tuning tn) {
+               int* __restrict__ max_row_len, unsigned* status, Tuning tn) {
   __shared__ int hist[SB_COUNT], base[SB_COUNT];
   __shared__ int rowbin[RA_ROWS], rowrank[RA_ROWS];
   __shared__ unsigned long long block_p;
@@ -123,6 +123,7 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
       acc += __shfl_sync(FULL, incl, 31);
     }
     if (lane == 0) {
+      if (re - rs > 0) atomicMax(max_row_len, re - rs);
       row_p[i] = acc;
       if (acc >= (1ll << 31)) atomicOr(status, ST_ROW_TOO_LONG);
       const int bin = sym_bin_of(acc, op.n, tn);
@@ -171,7 +172,6 @@ k_sym_warp(Operands op, const int* __restrict__ rows, int nrows, int* __restrict
   }
 }
 
-constexpr int BLOCK_CHUNK = 256;  // products per warp work unit in block-per-row kernels
 
 template <int LOG2T, int NT>
 __global__ void __launch_bounds__(NT)
@@ -193,8 +193,9 @@ k_sym_block(Operands op, const int* __restrict__ rows, int nrows,
     __syncthreads();
     SymHash f{keys, LOG2T, status, 0};
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
-    for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
-      warp_expand_range<false>(op, rs, re, c0, min(c0 + BLOCK_CHUNK, p), f, sc);
+    const int U = chunk_for(p, NW, 1 << 20);
+    for (int c0 = warp * U; c0 < p; c0 += NW * U)
+      warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
     const int u = warp_sum(f.nnew);
     if (lane == 0 && u) atomicAdd(&total, u);
     __syncthreads();
@@ -204,7 +205,6 @@ k_sym_block(Operands op, const int* __restrict__ rows, int nrows,
 }
 
 constexpr int LONG_THREADS = 1024;
-constexpr int LONG_CHUNK = 1024;  // products per warp work unit in long-row kernels
 
 // Exact nnz of long rows: presence bitmap of the row's columns in shared
 // memory, one window of `tn.sym_window` columns at a time. Also records the
@@ -213,38 +213,39 @@ __global__ void __launch_bounds__(LONG_THREADS)
 k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
            const long long* __restrict__ row_p, int* __restrict__ c_cnt,
            int* __restrict__ long_slot, int* __restrict__ chunk_cnt, int n_chunks,
-           unsigned* status, Tuning tn) {
+           int* __restrict__ scratch, int scratch_stride, unsigned* status, Tuning tn) {
   constexpr int NW = LONG_THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int total;
-  __shared__ int next_batch;
+  __shared__ long long scan_shm[33];
+  __shared__ int carry_shm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   unsigned* bits = reinterpret_cast<unsigned*>(smem + NW * sizeof(SegScratch));
+  int* seg_start = scratch + (size_t)blockIdx.x * scratch_stride;
   const int n = op.n;
   for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = rows[r];
     const int p = (int)row_p[i];
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    int* roff = seg_start + (re - rs);
     if (threadIdx.x == 0) { total = 0; long_slot[i] = r; }
     for (int w0 = 0; w0 < n; w0 += tn.sym_window) {
       const int wcols = min(n - w0, tn.sym_window);
       const int nw = (wcols + 31) >> 5;
       for (int t = threadIdx.x; t < nw; t += LONG_THREADS) bits[t] = 0u;
-      if (threadIdx.x == 0) next_batch = 0;
       __syncthreads();
       SymBits f{bits, w0, (unsigned)wcols, status};
       if (w0 == 0 && wcols == n) {
-        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
-          warp_expand_range<false>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
+        const int U = chunk_for(p, NW, 1 << 20);
+        for (int c0 = warp * U; c0 < p; c0 += NW * U)
+          warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
       } else {
-        for (;;) {
-          int jb = 0;
-          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
-          jb = __shfl_sync(FULL, jb, 0);
-          if (jb >= re) break;
-          warp_expand_restricted<false>(op, jb, re, w0, w0 + wcols, f, sc);
-        }
+        const int pw = block_restrict_row(op, rs, re, w0, w0 + wcols, seg_start, roff,
+                                          scan_shm, &carry_shm);
+        const int U = chunk_for(pw, NW, 1 << 20);
+        for (int c0 = warp * U; c0 < pw; c0 += NW * U)
+          warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, pw), f, sc);
       }
       __syncthreads();
       // chunk counts (w0 is a multiple of CHUNK_COLS)
@@ -385,10 +386,12 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
   if (threadIdx.x < NB_COUNT) hist[threadIdx.x] = 0;
   __syncthreads();
   int bin = -1, rank = 0;
+  bool listed = false;  // long rows go to the slice list, not a row list
   if (i < m) {
     const int o = c_cnt[i];
     bin = num_bin_of(o, row_p[i], tn);
     if (bin == NB_LONG) {
+      atomicAdd(&hist[NB_LONG], 1);
       const long long out0 = c_rowptr[i];
       if (o <= tn.slice_cap && n <= tn.slice_cols) {
         const int s = atomicAdd(slice_count, 1);
@@ -420,16 +423,16 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
           else atomicOr(status, ST_SLICE_OVERFLOW);
         }
       }
-      bin = -1;
     } else if (bin >= 0) {
       rank = atomicAdd(&hist[bin], 1);
+      listed = true;
     }
   }
   __syncthreads();
   if (threadIdx.x < NB_COUNT && hist[threadIdx.x])
     base[threadIdx.x] = atomicAdd(num_count + threadIdx.x, hist[threadIdx.x]);
   __syncthreads();
-  if (bin >= 0) num_rows[(size_t)bin * m + base[bin] + rank] = i;
+  if (listed) num_rows[(size_t)bin * m + base[bin] + rank] = i;
 }
 
 // ---------------------------------------------------------------------------
@@ -501,18 +504,19 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
     __syncthreads();
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     const bool fp64 = MODE == 1 && p > FP64_ROW_PARTIALS;
+    const int U = chunk_for(p, NW, 1 << 20);
     if (MODE == 0) {
       NumHashPlain f{keys, reinterpret_cast<float*>(vals), LOG2T, status};
-      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
-        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + U, p), f, sc);
     } else if (fp64) {
       NumHashF64 f{keys, reinterpret_cast<double*>(vals), LOG2T, status};
-      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
-        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + U, p), f, sc);
     } else {
       NumHashTwoSum f{keys, reinterpret_cast<float2*>(vals), LOG2T, status};
-      for (int c0 = warp * BLOCK_CHUNK; c0 < p; c0 += NW * BLOCK_CHUNK)
-        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + BLOCK_CHUNK, p), f, sc);
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + U, p), f, sc);
     }
     __syncthreads();
     bitonic_sort_kv<T, NT>(keys, vals, threadIdx.x, BlockSync());
@@ -543,20 +547,22 @@ template <int MODE>
 __global__ void __launch_bounds__(LONG_THREADS)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            const long long* __restrict__ row_p, int dir_words, int cap,
+           int* __restrict__ scratch, int scratch_stride,
            int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
   constexpr int NW = LONG_THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long scan_shm[33];
-  __shared__ int next_batch;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __shared__ int carry_shm;
+  const int warp = threadIdx.x >> 5;
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
   unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
+  int* seg_start = scratch + (size_t)blockIdx.x * scratch_stride;
   for (int s = blockIdx.x; s < nslices; s += gridDim.x) {
     const Slice sl = slices[s];
     const int i = sl.row;
-    const int p = (int)row_p[i];
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    int* roff = seg_start + (re - rs);
     const bool full = sl.lo == 0 && sl.hi == op.n;
     const int nw = (sl.hi - sl.lo + 31) >> 5;
     const int cnt = sl.cnt;
@@ -565,22 +571,21 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       continue;
     }
     for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(0u, 0u);
-    if (threadIdx.x == 0) next_batch = 0;
-    __syncthreads();
+    // products of the slice: the whole row, or its restriction to [lo, hi)
+    int p;
+    if (full) {
+      p = (int)row_p[i];
+      __syncthreads();
+    } else {
+      p = block_restrict_row(op, rs, re, sl.lo, sl.hi, seg_start, roff, scan_shm, &carry_shm);
+    }
+    const int U = chunk_for(p, NW, 1 << 20);
     // pass 1: presence bits
     {
       LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
-      if (full) {
-        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
-          warp_expand_range<false>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
-      } else {
-        for (;;) {
-          int jb = 0;
-          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
-          jb = __shfl_sync(FULL, jb, 0);
-          if (jb >= re) break;
-          warp_expand_restricted<false>(op, jb, re, sl.lo, sl.hi, f, sc);
-        }
+      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
+        if (full) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     }
     __syncthreads();
@@ -595,7 +600,6 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       long long run = block_excl_scan64(local, scan_shm, tot);
       for (int q = 0; q < per; ++q)
         if (w0 + q < nw) { dir[w0 + q].y = (unsigned)run; run += __popc(dir[w0 + q].x); }
-      if (threadIdx.x == 0) next_batch = 0;
     }
     if (tot != cnt) {  // block-uniform: slots would not fit the slice
       if (threadIdx.x == 0) atomicOr(status, ST_COUNT_MISMATCH);
@@ -613,31 +617,15 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     // pass 2: values
     if (MODE == 0) {
       LongValPlain f{dir, reinterpret_cast<float*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
-      if (full) {
-        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
-          warp_expand_range<true>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
-      } else {
-        for (;;) {
-          int jb = 0;
-          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
-          jb = __shfl_sync(FULL, jb, 0);
-          if (jb >= re) break;
-          warp_expand_restricted<true>(op, jb, re, sl.lo, sl.hi, f, sc);
-        }
+      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
+        if (full) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     } else {
       LongValF64 f{dir, reinterpret_cast<double*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
-      if (full) {
-        for (int c0 = warp * LONG_CHUNK; c0 < p; c0 += NW * LONG_CHUNK)
-          warp_expand_range<true>(op, rs, re, c0, min(c0 + LONG_CHUNK, p), f, sc);
-      } else {
-        for (;;) {
-          int jb = 0;
-          if (lane == 0) jb = rs + 32 * atomicAdd(&next_batch, 1);
-          jb = __shfl_sync(FULL, jb, 0);
-          if (jb >= re) break;
-          warp_expand_restricted<true>(op, jb, re, sl.lo, sl.hi, f, sc);
-        }
+      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
+        if (full) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     }
     __syncthreads();

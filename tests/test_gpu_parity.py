@@ -83,14 +83,14 @@ def test_empty_product():
 
 
 def test_rmat_all_bins():
-    A = W.rmat(13, 16, 1)
+    A = W.rmat(14, 16, 1)
     _, _, stats = check(A, A)
     assert stats["rows_per_symbolic_bin"][8] > 0, stats
     assert stats["rows_per_numeric_bin"][8] > 0, stats
 
 
 def test_rmat_all_bins_compensated():
-    A = W.rmat(13, 16, 2)
+    A = W.rmat(14, 16, 2)
     check(A, A, sg.COMPENSATED)
 
 
