@@ -62,6 +62,24 @@ typedef struct spgemm_stats {
     long long kernel_launches;         /* engine kernels launched by the handle so far */
 } spgemm_stats;
 
+/* Bin thresholds and slice shapes of the engine (spgemm_get_tuning returns
+ * the defaults of a new handle). Row i has P_i partial products and nnz_i
+ * outputs; a "long" row is handled by column-slice blocks with a presence
+ * bitmap instead of a shared-memory hash table. */
+typedef struct spgemm_tuning {
+    int warp_p_max_sym;   /* symbolic: one warp per row when P_i <= this */
+    int warp_p_max_num;   /* numeric: one warp per row when P_i <= this */
+    int long_p_sym;       /* symbolic: bitmap (long) path when P_i > this (<= 4096) */
+    int long_o_num;       /* numeric: slice (long) path when nnz_i > this
+                             (>= long_p_sym, <= 4096) */
+    int slice_cap;        /* max outputs per numeric slice; 0 = shared-memory limit */
+    int slice_cols;       /* max columns per numeric slice (multiple of 2048) */
+    int sym_window;       /* columns per symbolic bitmap window (multiple of 2048,
+                             <= 2^20) */
+    int keep_bitmaps;     /* 1: keep the long rows' symbolic bitmaps (device memory
+                             permitting) so the numeric pass skips rebuilding them */
+} spgemm_tuning;
+
 /* Library version string. */
 const char* spgemm_version(void);
 /* Human-readable text of a status code. */
@@ -76,6 +94,10 @@ int spgemm_destroy(spgemm_handle_t handle);
 int spgemm_set_stream(spgemm_handle_t handle, void* stream);
 /* Select SPGEMM_PRECISION_PLAIN or SPGEMM_PRECISION_COMPENSATED. */
 int spgemm_set_precision(spgemm_handle_t handle, int precision);
+/* Read / replace the handle's tuning (validated; SPGEMM_ERR_INVALID if a
+ * field breaks a documented range). */
+int spgemm_get_tuning(spgemm_handle_t handle, spgemm_tuning* out);
+int spgemm_set_tuning(spgemm_handle_t handle, const spgemm_tuning* in);
 /* Text of the handle's last error ("" if none). */
 const char* spgemm_last_error(spgemm_handle_t handle);
 

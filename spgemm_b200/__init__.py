@@ -56,6 +56,16 @@ class COO(C.Structure):
                 ("num_rows", C.c_int), ("type", C.c_bool)]
 
 
+class Tuning(C.Structure):
+    """spgemm_tuning (include/spgemm_b200.h)."""
+    _fields_ = [("warp_p_max_sym", C.c_int), ("warp_p_max_num", C.c_int),
+                ("long_p_sym", C.c_int), ("long_o_num", C.c_int), ("slice_cap", C.c_int),
+                ("slice_cols", C.c_int), ("sym_window", C.c_int), ("keep_bitmaps", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Stats(C.Structure):
     _fields_ = [("intermediate_products", C.c_longlong), ("nnz_c", C.c_longlong),
                 ("rows_per_symbolic_bin", C.c_int * 16), ("rows_per_numeric_bin", C.c_int * 16),
@@ -91,6 +101,8 @@ def lib():
         L.spgemm_get_result.argtypes = [C.POINTER(CM)]
         L.spgemm_set_verbose.argtypes = [C.c_int]
         L.spgemm_set_exit_on_error.argtypes = [C.c_int]
+        L.spgemm_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.spgemm_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.spgemm_set_profiling.argtypes = [vp, C.c_int]
         L.spgemm_reset_kernel_times.argtypes = [vp]
         L.spgemm_get_kernel_times.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
@@ -189,6 +201,21 @@ class Handle:
                 "rows_per_symbolic_bin": list(s.rows_per_symbolic_bin)[:9],
                 "rows_per_numeric_bin": list(s.rows_per_numeric_bin)[:9],
                 "long_row_slices": s.long_row_slices, "kernel_launches": s.kernel_launches}
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        self._check(lib().spgemm_get_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        """Change tuning fields by name (others keep their current value)."""
+        t = Tuning()
+        self._check(lib().spgemm_get_tuning(self._h, C.byref(t)))
+        for k, v in kw.items():
+            if not hasattr(t, k):
+                raise KeyError(k)
+            setattr(t, k, int(v))
+        self._check(lib().spgemm_set_tuning(self._h, C.byref(t)))
 
     def set_profiling(self, on: bool = True):
         self._check(lib().spgemm_set_profiling(self._h, 1 if on else 0))

@@ -92,6 +92,34 @@ int spgemm_set_precision(spgemm_handle_t h, int precision) {
   return h->eng.set_precision(precision);
 }
 
+int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
+  if (!h || !out) return SPGEMM_ERR_INVALID;
+  const sg::Tuning& t = h->eng.tuning();
+  out->warp_p_max_sym = t.warp_p_max_sym;
+  out->warp_p_max_num = t.warp_p_max_num;
+  out->long_p_sym = t.long_p_sym;
+  out->long_o_num = t.long_o_num;
+  out->slice_cap = t.slice_cap;
+  out->slice_cols = t.slice_cols;
+  out->sym_window = t.sym_window;
+  out->keep_bitmaps = t.keep_bitmaps;
+  return SPGEMM_OK;
+}
+
+int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
+  if (!h || !in) return SPGEMM_ERR_INVALID;
+  sg::Tuning t;
+  t.warp_p_max_sym = in->warp_p_max_sym;
+  t.warp_p_max_num = in->warp_p_max_num;
+  t.long_p_sym = in->long_p_sym;
+  t.long_o_num = in->long_o_num;
+  t.slice_cap = in->slice_cap;
+  t.slice_cols = in->slice_cols;
+  t.sym_window = in->sym_window;
+  t.keep_bitmaps = in->keep_bitmaps ? 1 : 0;
+  return h->eng.set_tuning(t);
+}
+
 const char* spgemm_last_error(spgemm_handle_t h) {
   return h ? h->eng.last_error().c_str() : "null handle";
 }

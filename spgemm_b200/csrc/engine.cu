@@ -40,7 +40,8 @@ Tuning default_tuning() {
   t.warp_p_max_num = 2048;
   t.long_p_sym = 4096;
   t.long_o_num = 4096;
-  t.slice_cap = 16384;      // recomputed per product from the shared-memory budget
+  t.slice_cap = 0;          // 0: as many as the shared-memory budget allows
+  t.keep_bitmaps = 1;
   t.slice_cols = 1 << 18;
   t.sym_window = 1 << 20;
   return t;
@@ -103,7 +104,7 @@ int Engine::prof_collect() {
 Engine::~Engine() {
   DevBuf* all[] = {&a_rowptr_, &a_col_, &a_val_, &cursor_, &aoff_, &row_p_, &c_cnt_,
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
-                   &chunk_cnt_, &slices_buf_, &counters_, &restrict_scratch_, &out_rowptr_,
+                   &chunk_cnt_, &slices_buf_, &counters_, &restrict_scratch_, &bitmaps_, &out_rowptr_,
                    &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
   for (DevBuf& b : stage_) b.release();
@@ -135,6 +136,9 @@ int Engine::set_tuning(const Tuning& t) {
   if (t.sym_window < CHUNK_COLS || t.sym_window % CHUNK_COLS || t.sym_window > (1 << 20))
     return fail(1, "tuning: sym_window");
   if (t.warp_p_max_sym < 0 || t.warp_p_max_num < 0) return fail(1, "tuning: warp limits");
+  if (t.slice_cap != 0 && t.slice_cap < CHUNK_COLS)
+    return fail(1, "tuning: slice_cap must be 0 (auto) or >= 2048");
+  if (t.long_p_sym < 1) return fail(1, "tuning: long_p_sym");
   tn_ = t;
   return 0;
 }
@@ -350,6 +354,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
     const size_t fixed = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + dir_bytes;
     long long cap = (long long)((LONG_SMEM_BUDGET - fixed) / vb);
     cap = std::min<long long>(cap, 1 << 20);
+    if (tn_.slice_cap > 0) cap = std::min<long long>(cap, tn_.slice_cap);
     tr.slice_cap = (int)cap;
     tn_run_slice_cap_ = tr.slice_cap;
   }
@@ -384,6 +389,7 @@ int Engine::launch_symbolic_bins() {
   const long long* row_p = row_p_.as<long long>();
   const int* rows = sym_rows_.as<int>();
   constexpr int WPB = SW_THREADS / 32;
+  bitmap_words_ = 0;
   // long rows first: they are the heaviest work items
   if (sym_counts_[SB_LONG] > 0) {
     const int win = std::min(n_, tn_.sym_window);
@@ -396,10 +402,22 @@ int Engine::launch_symbolic_bins() {
       SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
     else
       SG_CK(restrict_scratch_.ensure(16), "alloc restrict scratch");
+    // Keep the long rows' presence bitmaps for the numeric pass when they fit
+    // in a modest share of free device memory; otherwise it rebuilds them.
+    if (tn_.keep_bitmaps) {
+      const size_t words = (size_t)(n_ + 31) / 32;
+      const size_t want = words * 4 * (size_t)cnt;
+      size_t free_b = 0, total_b = 0;
+      cudaMemGetInfo(&free_b, &total_b);
+      const size_t budget = std::min<size_t>((size_t)16 << 30, (free_b + bitmaps_.bytes) / 4);
+      if (want <= budget && bitmaps_.ensure(want) == cudaSuccess) bitmap_words_ = (int)words;
+      cudaGetLastError();  // a failed optional allocation is not an error
+    }
     prof_begin("k_sym_long");
     k_sym_long<<<grid, LONG_THREADS, smem, stream_>>>(
         op, rows + (size_t)SB_LONG * m, cnt, row_p, c_cnt, long_slot_.as<int>(),
-        chunk_cnt_.as<int>(), n_chunks_, restrict_scratch_.as<int>(), stride, status, tn_);
+        chunk_cnt_.as<int>(), n_chunks_, restrict_scratch_.as<int>(), stride,
+        bitmaps_.as<unsigned>(), bitmap_words_, status, tn_);
     SG_LAUNCHED("k_sym_long");
   }
 #define SG_SYM_WARP(L)                                                                    \
@@ -440,7 +458,8 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
                                const long long* c_rowptr, int* c_col, float* c_val,
                                unsigned* status, cudaStream_t stream, int sms, int n,
                                int slice_cols, int slice_cap, DevBuf& scratch,
-                               int max_row_len, long long& launches);
+                               int max_row_len, const unsigned* bitmaps, int bitmap_words,
+                               const int* long_slot, long long& launches);
 
 int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
@@ -466,12 +485,16 @@ int Engine::launch_numeric_bins(int* c_col, float* c_val) {
                                   slices_buf_.as<Slice>(), &dc->slice_count,
                                   row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
                                   c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                  tn_run_slice_cap_, restrict_scratch_, max_row_len_, launches_);
+                                  tn_run_slice_cap_, restrict_scratch_, max_row_len_,
+                                  bitmaps_.as<unsigned>(), bitmap_words_, long_slot_.as<int>(),
+                                  launches_);
   return launch_numeric_impl<1>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
                                 slices_buf_.as<Slice>(), &dc->slice_count,
                                 row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
                                 c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                tn_run_slice_cap_, restrict_scratch_, max_row_len_, launches_);
+                                tn_run_slice_cap_, restrict_scratch_, max_row_len_,
+                                  bitmaps_.as<unsigned>(), bitmap_words_, long_slot_.as<int>(),
+                                  launches_);
 }
 
 template <class K>
@@ -499,7 +522,8 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
                                const long long* c_rowptr, int* c_col, float* c_val,
                                unsigned* status, cudaStream_t stream, int sms, int n,
                                int slice_cols, int slice_cap, DevBuf& scratch,
-                               int max_row_len, long long& launches) {
+                               int max_row_len, const unsigned* bitmaps, int bitmap_words,
+                               const int* long_slot, long long& launches) {
   constexpr int WPB = SW_THREADS / 32;
   constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
   if (nslices > 0) {
@@ -513,8 +537,8 @@ static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, i
     SG_CKE(scratch.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
     E.prof_begin("k_num_long");
     k_num_long<MODE><<<grid, LONG_THREADS, smem, stream>>>(
-        op, slices, nslices, row_p, dir_words, slice_cap, scratch.as<int>(), stride, c_col,
-        c_val, status);
+        op, slices, nslices, row_p, dir_words, slice_cap, scratch.as<int>(), stride, bitmaps,
+        bitmap_words, long_slot, c_col, c_val, status);
     SG_LAUNCHED_E("k_num_long");
   }
 #define SG_NUM_WARP(L)                                                                       \

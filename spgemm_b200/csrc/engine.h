@@ -124,7 +124,8 @@ class Engine {
   DevBuf a_rowptr_, a_col_, a_val_, cursor_, aoff_;
   DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
   DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_;
-  DevBuf counters_, restrict_scratch_;
+  DevBuf counters_, restrict_scratch_, bitmaps_;
+  int bitmap_words_ = 0;  // per long row; 0 when the bitmaps are not kept
   int max_row_len_ = 0;
   DevBuf out_rowptr_, out_col_, out_val_;
   DevBuf stage_[6];

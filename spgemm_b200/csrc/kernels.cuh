@@ -58,9 +58,10 @@ struct Tuning {
   int warp_p_max_num;   // numeric: warp-per-row only when P_i <= this
   int long_p_sym;       // symbolic: bitmap path when P_i > this
   int long_o_num;       // numeric: slice path when nnz_i > this (>= long_p_sym)
-  int slice_cap;        // max outputs of one numeric long slice
+  int slice_cap;        // max outputs of one numeric long slice (0: smem budget)
   int slice_cols;       // max columns of one numeric long slice (multiple of 2048)
   int sym_window;       // columns per symbolic bitmap window (multiple of 2048)
+  int keep_bitmaps;     // keep long rows' symbolic bitmaps for the numeric pass
 };
 
 __host__ __device__ inline int ceil_log2_ll(long long v) {
@@ -186,11 +187,13 @@ __device__ __forceinline__ void run_segments(int cnt, int bstart, int len, float
 }
 
 // Products per warp work unit when the warps of a block share one row of
-// `p` products: about 8 units per warp, a multiple of 32, at least 64.
+// `p` products. Units are equal slices of the row's flattened product
+// sequence, so one unit per warp is already balanced; each unit costs one
+// binary search to find its first entry.
 __device__ __forceinline__ int chunk_for(long long p, int nwarps, int max_chunk) {
-  long long u = (p + nwarps * 8 - 1) / (nwarps * 8);
+  long long u = (p + nwarps - 1) / nwarps;
   u = (u + 31) & ~31ll;
-  if (u < 64) u = 64;
+  if (u < 32) u = 32;
   if (u > max_chunk) u = max_chunk;
   return (int)u;
 }

@@ -213,7 +213,8 @@ __global__ void __launch_bounds__(LONG_THREADS)
 k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
            const long long* __restrict__ row_p, int* __restrict__ c_cnt,
            int* __restrict__ long_slot, int* __restrict__ chunk_cnt, int n_chunks,
-           int* __restrict__ scratch, int scratch_stride, unsigned* status, Tuning tn) {
+           int* __restrict__ scratch, int scratch_stride, unsigned* __restrict__ bitmaps,
+           int bitmap_words, unsigned* status, Tuning tn) {
   constexpr int NW = LONG_THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int total;
@@ -248,6 +249,11 @@ k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
           warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, pw), f, sc);
       }
       __syncthreads();
+      // keep the presence bitmap for the numeric pass (when memory allows)
+      if (bitmap_words > 0) {
+        unsigned* dst = bitmaps + (size_t)r * bitmap_words + (w0 >> 5);
+        for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dst[t] = bits[t];
+      }
       // chunk counts (w0 is a multiple of CHUNK_COLS)
       const int nchunk_w = (nw + CHUNK_WORDS - 1) / CHUNK_WORDS;
       for (int c = warp; c < nchunk_w; c += NW) {
@@ -548,6 +554,8 @@ __global__ void __launch_bounds__(LONG_THREADS)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            const long long* __restrict__ row_p, int dir_words, int cap,
            int* __restrict__ scratch, int scratch_stride,
+           const unsigned* __restrict__ bitmaps, int bitmap_words,
+           const int* __restrict__ long_slot,
            int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
   constexpr int NW = LONG_THREADS / 32;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -570,7 +578,13 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
       continue;
     }
-    for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(0u, 0u);
+    const bool have_bits = bitmap_words > 0;
+    if (have_bits) {  // the symbolic pass kept this row's presence bitmap
+      const unsigned* src = bitmaps + (size_t)long_slot[i] * bitmap_words + (sl.lo >> 5);
+      for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(__ldg(src + t), 0u);
+    } else {
+      for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(0u, 0u);
+    }
     // products of the slice: the whole row, or its restriction to [lo, hi)
     int p;
     if (full) {
@@ -580,15 +594,15 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       p = block_restrict_row(op, rs, re, sl.lo, sl.hi, seg_start, roff, scan_shm, &carry_shm);
     }
     const int U = chunk_for(p, NW, 1 << 20);
-    // pass 1: presence bits
-    {
+    // pass 1: presence bits (only when the bitmap was not kept)
+    if (!have_bits) {
       LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
         if (full) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
+      __syncthreads();
     }
-    __syncthreads();
     // ranks: exclusive scan of popcounts over the nw directory words
     long long tot;
     {

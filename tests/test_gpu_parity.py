@@ -149,3 +149,39 @@ def test_repeat_calls_reuse_workspace():
         C = h.multiply_host(B.to_csc(), B)
         ref = ref_product(B, B)
         assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+
+
+TUNINGS = [
+    dict(keep_bitmaps=0),                                   # numeric rebuilds long-row bitmaps
+    dict(slice_cap=2048, slice_cols=8192),                  # many column slices per long row
+    dict(warp_p_max_sym=0, warp_p_max_num=0),               # every short row block-per-row
+    dict(long_p_sym=256, long_o_num=256),                   # mid rows take the long path
+    dict(sym_window=4096, slice_cols=4096, slice_cap=2048,  # multi-window symbolic pass,
+         keep_bitmaps=0),                                   # restricted numeric slices
+]
+
+
+@pytest.mark.parametrize("tuning", TUNINGS, ids=lambda t: ",".join(f"{k}={v}" for k, v in t.items()))
+@pytest.mark.parametrize("precision", [sg.PLAIN, sg.COMPENSATED])
+def test_tuning_overrides(tuning, precision):
+    A = W.rmat(14, 16, 5)
+    ref = ref_product(A, A)
+    with sg.Handle(precision) as h:
+        h.set_tuning(**tuning)
+        C = h.multiply_host(A.to_csc(), A)
+        stats = h.stats()
+    assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+    tol = plain_tolerance(ref) if precision == sg.PLAIN else compensated_tolerance(ref)
+    assert_values_close(C.val, ref, tol)
+    if "slice_cap" in tuning:
+        assert stats["long_row_slices"] > stats["rows_per_numeric_bin"][8], stats
+
+
+def test_bad_tuning_rejected():
+    with sg.Handle() as h:
+        with pytest.raises(sg.SpgemmError):
+            h.set_tuning(long_o_num=100, long_p_sym=200)
+        with pytest.raises(sg.SpgemmError):
+            h.set_tuning(slice_cols=1000)
+        with pytest.raises(sg.SpgemmError):
+            h.set_tuning(long_p_sym=5000)
