@@ -78,6 +78,10 @@ typedef struct spgemm_tuning {
                              <= 2^20) */
     int keep_bitmaps;     /* 1: keep the long rows' symbolic bitmaps (device memory
                              permitting) so the numeric pass skips rebuilding them */
+    int mid_o_min;        /* numeric: rows with mid_o_min < nnz_i <= long_o_num whose
+                             column span is at most mid_cols take the bitmap kernel
+                             instead of a hash table + sort */
+    int mid_cols;         /* (<= 2^18) */
 } spgemm_tuning;
 
 /* Library version string. */

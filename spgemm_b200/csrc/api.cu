@@ -103,6 +103,8 @@ int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
   out->slice_cols = t.slice_cols;
   out->sym_window = t.sym_window;
   out->keep_bitmaps = t.keep_bitmaps;
+  out->mid_o_min = t.mid_o_min;
+  out->mid_cols = t.mid_cols;
   return SPGEMM_OK;
 }
 
@@ -117,6 +119,8 @@ int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
   t.slice_cols = in->slice_cols;
   t.sym_window = in->sym_window;
   t.keep_bitmaps = in->keep_bitmaps ? 1 : 0;
+  t.mid_o_min = in->mid_o_min;
+  t.mid_cols = in->mid_cols;
   return h->eng.set_tuning(t);
 }
 

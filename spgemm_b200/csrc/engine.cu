@@ -42,6 +42,8 @@ Tuning default_tuning() {
   t.long_o_num = 4096;
   t.slice_cap = 0;          // 0: as many as the shared-memory budget allows
   t.keep_bitmaps = 1;
+  t.mid_o_min = 256;
+  t.mid_cols = 1 << 18;
   t.slice_cols = 1 << 18;
   t.sym_window = 1 << 20;
   return t;
@@ -104,7 +106,8 @@ int Engine::prof_collect() {
 Engine::~Engine() {
   DevBuf* all[] = {&a_rowptr_, &a_col_, &a_val_, &cursor_, &aoff_, &row_p_, &c_cnt_,
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
-                   &chunk_cnt_, &slices_buf_, &counters_, &restrict_scratch_, &bitmaps_, &out_rowptr_,
+                   &chunk_cnt_, &slices_buf_, &mid_slices_, &row_span_, &counters_, &restrict_scratch_,
+                   &bitmaps_, &out_rowptr_,
                    &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
   for (DevBuf& b : stage_) b.release();
@@ -139,6 +142,8 @@ int Engine::set_tuning(const Tuning& t) {
   if (t.slice_cap != 0 && t.slice_cap < CHUNK_COLS)
     return fail(1, "tuning: slice_cap must be 0 (auto) or >= 2048");
   if (t.long_p_sym < 1) return fail(1, "tuning: long_p_sym");
+  if (t.mid_o_min < 0 || t.mid_cols < 0 || t.mid_cols > (1 << 18))
+    return fail(1, "tuning: mid_o_min >= 0 and 0 <= mid_cols <= 2^18");
   tn_ = t;
   return 0;
 }
@@ -305,12 +310,14 @@ int Engine::analyze(const cm& A, const cm& B) {
   SG_CK(aoff_.ensure(sizeof(int) * (size_t)std::max(nnz_a, 1)), "alloc aoff");
   SG_CK(row_p_.ensure(sizeof(long long) * (size_t)std::max(m, 1)), "alloc row_p");
   SG_CK(sym_rows_.ensure(sizeof(int) * (size_t)SB_COUNT * std::max(m, 1)), "alloc sym_rows");
+  SG_CK(row_span_.ensure(sizeof(int2) * (size_t)std::max(m, 1)), "alloc row spans");
   op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_};
   if (m > 0) {
     prof_begin("k_row_analysis");
     k_row_analysis<<<(m + RA_ROWS - 1) / RA_ROWS, RA_THREADS, 0, stream_>>>(
         op_, aoff_.as<int>(), row_p_.as<long long>(), c_cnt_.as<int>(), dc->sym_count,
-        sym_rows_.as<int>(), &dc->p_total, &dc->max_row_len, &dc->status, tn_);
+        sym_rows_.as<int>(), &dc->p_total, &dc->max_row_len, row_span_.as<int2>(), &dc->status,
+        tn_);
     SG_LAUNCHED("k_row_analysis");
   }
   SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
@@ -343,15 +350,14 @@ int Engine::symbolic_pass(long long* nnz_c) {
   // ---- row pointers + numeric binning ----
   if (int r = scan_counts(c_cnt_.as<int>(), m, c_rowptr64_.as<long long>())) return r;
   SG_CK(num_rows_.ensure(sizeof(int) * (size_t)NB_COUNT * std::max(m, 1)), "alloc num_rows");
-  const long long slice_cap_rows = (long long)n_long_sym_ * std::max(n_chunks_, 1);
-  SG_CK(slices_buf_.ensure(sizeof(Slice) * (size_t)std::max(slice_cap_rows, 1ll)), "alloc slices");
-  // long-slice output capacity from the shared-memory budget
+  big_capacity_ = (long long)n_long_sym_ * std::max(n_chunks_, 1);
+  SG_CK(slices_buf_.ensure(sizeof(Slice) * (size_t)std::max(big_capacity_, 1ll)), "alloc slices");
+  SG_CK(mid_slices_.ensure(sizeof(Slice) * (size_t)std::max(m, 1)), "alloc mid slices");
+  // output capacity of one big slice: what the shared-memory budget leaves
   Tuning tr = tn_;
   {
     const size_t vb = precision_ == 1 ? 8 : 4;
-    const int width = std::min(n_, tr.slice_cols);
-    const size_t dir_bytes = (size_t)((width + 31) / 32) * sizeof(uint2);
-    const size_t fixed = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + dir_bytes;
+    const size_t fixed = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes();
     long long cap = (long long)((LONG_SMEM_BUDGET - fixed) / vb);
     cap = std::min<long long>(cap, 1 << 20);
     if (tn_.slice_cap > 0) cap = std::min<long long>(cap, tn_.slice_cap);
@@ -362,8 +368,9 @@ int Engine::symbolic_pass(long long* nnz_c) {
     prof_begin("k_num_bin");
     k_num_bin<<<(m + NBIN_THREADS - 1) / NBIN_THREADS, NBIN_THREADS, 0, stream_>>>(
         m, n_, c_cnt_.as<int>(), row_p_.as<long long>(), c_rowptr64_.as<long long>(),
-        dc->num_count, num_rows_.as<int>(), long_slot_.as<int>(), chunk_cnt_.as<int>(),
-        n_chunks_, slices_buf_.as<Slice>(), &dc->slice_count, (int)slice_cap_rows,
+        row_span_.as<int2>(), dc->num_count, num_rows_.as<int>(), chunk_cnt_.as<int>(),
+        n_chunks_, long_slot_.as<int>(), slices_buf_.as<Slice>(), &dc->slice_count,
+        (int)big_capacity_, mid_slices_.as<Slice>(), &dc->mid_count, bitmap_words_ > 0 ? 1 : 0,
         &dc->status, tr);
     SG_LAUNCHED("k_num_bin");
   }
@@ -374,6 +381,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
   nnz_c_ = host_counters_->grand_total;
   for (int b = 0; b < NB_COUNT; ++b) num_counts_[b] = host_counters_->num_count[b];
   nslices_ = host_counters_->slice_count;
+  nmid_ = host_counters_->mid_count;
   if (nnz_c_ > 2147483647ll)
     return fail(4, "nnz(C) = " + std::to_string(nnz_c_) + " exceeds the int32 range of cm");
   if (nnz_c) *nnz_c = nnz_c_;
@@ -451,16 +459,6 @@ int Engine::launch_symbolic_bins() {
   return 0;
 }
 
-template <int MODE>
-static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, int m,
-                               const int* counts, int nslices, const Slice* slices,
-                               const int* nslices_dev, const long long* row_p,
-                               const long long* c_rowptr, int* c_col, float* c_val,
-                               unsigned* status, cudaStream_t stream, int sms, int n,
-                               int slice_cols, int slice_cap, DevBuf& scratch,
-                               int max_row_len, const unsigned* bitmaps, int bitmap_words,
-                               const int* long_slot, long long& launches);
-
 int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
   if (!c_rowptr || (nnz_c_ > 0 && (!c_col || !c_val))) return fail(1, "null output pointer");
@@ -479,99 +477,90 @@ int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
 }
 
 int Engine::launch_numeric_bins(int* c_col, float* c_val) {
-  DevCounters* dc = counters_.as<DevCounters>();
-  if (precision_ == 0)
-    return launch_numeric_impl<0>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
-                                  slices_buf_.as<Slice>(), &dc->slice_count,
-                                  row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
-                                  c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                  tn_run_slice_cap_, restrict_scratch_, max_row_len_,
-                                  bitmaps_.as<unsigned>(), bitmap_words_, long_slot_.as<int>(),
-                                  launches_);
-  return launch_numeric_impl<1>(*this, op_, num_rows_.as<int>(), m_, num_counts_, nslices_,
-                                slices_buf_.as<Slice>(), &dc->slice_count,
-                                row_p_.as<long long>(), c_rowptr64_.as<long long>(), c_col,
-                                c_val, &dc->status, stream_, sms_, n_, tn_.slice_cols,
-                                tn_run_slice_cap_, restrict_scratch_, max_row_len_,
-                                  bitmaps_.as<unsigned>(), bitmap_words_, long_slot_.as<int>(),
-                                  launches_);
+  return precision_ == 0 ? launch_numeric_mode<0>(c_col, c_val)
+                         : launch_numeric_mode<1>(c_col, c_val);
 }
 
-template <class K>
-static cudaError_t set_smem(K kernel, size_t bytes) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+size_t Engine::big_dir_bytes() const {
+  return (size_t)((std::min(n_, tn_.slice_cols) + 31) / 32) * sizeof(uint2);
 }
-
-#define SG_CKE(call, what)                                  \
-  do {                                                      \
-    cudaError_t e__ = (call);                               \
-    if (e__ != cudaSuccess) return E.cuda_fail(e__, what);  \
-  } while (0)
-#define SG_LAUNCHED_E(what)                                 \
-  do {                                                      \
-    ++launches;                                             \
-    E.prof_end();                                           \
-    cudaError_t e__ = cudaGetLastError();                   \
-    if (e__ != cudaSuccess) return E.cuda_fail(e__, what);  \
-  } while (0)
 
 template <int MODE>
-static int launch_numeric_impl(Engine& E, const Operands& op, const int* rows, int m,
-                               const int* counts, int nslices, const Slice* slices,
-                               const int* nslices_dev, const long long* row_p,
-                               const long long* c_rowptr, int* c_col, float* c_val,
-                               unsigned* status, cudaStream_t stream, int sms, int n,
-                               int slice_cols, int slice_cap, DevBuf& scratch,
-                               int max_row_len, const unsigned* bitmaps, int bitmap_words,
-                               const int* long_slot, long long& launches) {
+int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   constexpr int WPB = SW_THREADS / 32;
+  constexpr int MID_THREADS = 512;
   constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
-  if (nslices > 0) {
-    const int width = std::min(n, slice_cols);
+  const Operands op = op_;
+  const int m = m_;
+  const int* rows = num_rows_.as<int>();
+  const long long* row_p = row_p_.as<long long>();
+  const long long* c_rowptr = c_rowptr64_.as<long long>();
+  unsigned* status = &counters_.as<DevCounters>()->status;
+  const int stride = 2 * max_row_len_ + 2;
+  // big bitmap slices (long rows), one 1024-thread block per SM
+  if (nslices_ > 0) {
+    const int dir_words = (int)(big_dir_bytes() / sizeof(uint2));
+    const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes() +
+                        (size_t)tn_run_slice_cap_ * (MODE ? 8 : 4);
+    SG_CK(smem_attr(k_num_long<MODE, LONG_THREADS>, smem), "smem attr k_num_long");
+    const int grid = blocks_for(nslices_, 1, (long long)sms_ * 2);
+    SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
+    prof_begin("k_num_long");
+    k_num_long<MODE, LONG_THREADS><<<grid, LONG_THREADS, smem, stream_>>>(
+        op, slices_buf_.as<Slice>(), nslices_, row_p, dir_words, tn_run_slice_cap_,
+        restrict_scratch_.as<int>(), stride, bitmaps_.as<unsigned>(), bitmap_words_,
+        long_slot_.as<int>(), c_col, c_val, status);
+    SG_LAUNCHED("k_num_long");
+  }
+  // mid bitmap slices: whole rows of at most long_o_num outputs, 512 threads
+  if (nmid_ > 0) {
+    const int width = std::min(n_, tn_.mid_cols) + 32;  // + alignment of lo down to 32
     const int dir_words = (width + 31) / 32;
-    const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES +
-                        (size_t)dir_words * sizeof(uint2) + (size_t)slice_cap * (MODE ? 8 : 4);
-    SG_CKE(set_smem(k_num_long<MODE>, smem), "smem attr k_num_long");
-    const int grid = blocks_for(nslices, 1, (long long)sms * 2);
-    const int stride = 2 * max_row_len + 2;
-    SG_CKE(scratch.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
-    E.prof_begin("k_num_long");
-    k_num_long<MODE><<<grid, LONG_THREADS, smem, stream>>>(
-        op, slices, nslices, row_p, dir_words, slice_cap, scratch.as<int>(), stride, bitmaps,
-        bitmap_words, long_slot, c_col, c_val, status);
-    SG_LAUNCHED_E("k_num_long");
+    const size_t smem = (MID_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)dir_words * sizeof(uint2) +
+                        (size_t)tn_.long_o_num * (MODE ? 8 : 4);
+    SG_CK(smem_attr(k_num_long<MODE, MID_THREADS>, smem), "smem attr k_num_long mid");
+    const int grid = blocks_for(nmid_, 1, (long long)sms_ * 4);
+    prof_begin("k_num_mid");
+    k_num_long<MODE, MID_THREADS><<<grid, MID_THREADS, smem, stream_>>>(
+        op, mid_slices_.as<Slice>(), nmid_, row_p, dir_words, tn_.long_o_num,
+        restrict_scratch_.as<int>(), 0, bitmaps_.as<unsigned>(), bitmap_words_,
+        long_slot_.as<int>(), c_col, c_val, status);
+    SG_LAUNCHED("k_num_mid");
   }
 #define SG_NUM_WARP(L)                                                                       \
   {                                                                                           \
-    const int b = L - 6, cnt = counts[b];                                                     \
+    const int b = L - 6, cnt = num_counts_[b];                                                \
     if (cnt > 0) {                                                                            \
       const size_t smem = WPB * ((size_t(1) << L) * (VB + 4) + SEG_SCRATCH_BYTES);            \
-      SG_CKE(set_smem(k_num_warp<L, MODE>, smem), "smem attr k_num_warp");                    \
-      E.prof_begin("k_num_warp<" #L ">");                                                          \
-      k_num_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms * 8), SW_THREADS, smem,       \
-                            stream>>>(op, rows + (size_t)b * m, cnt, c_rowptr, c_col, c_val,  \
-                                      status);                                                \
-      SG_LAUNCHED_E("k_num_warp");                                                            \
+      SG_CK(smem_attr(k_num_warp<L, MODE>, smem), "smem attr k_num_warp");                    \
+      prof_begin("k_num_warp<" #L ">");                                                        \
+      k_num_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms_ * 8), SW_THREADS, smem,      \
+                            stream_>>>(op, rows + (size_t)b * m, cnt, c_rowptr, c_col, c_val, \
+                                       status);                                               \
+      SG_LAUNCHED("k_num_warp");                                                              \
     }                                                                                         \
   }
   SG_NUM_WARP(6) SG_NUM_WARP(7) SG_NUM_WARP(8) SG_NUM_WARP(9)
 #undef SG_NUM_WARP
 #define SG_NUM_BLOCK(L, NT)                                                                  \
   {                                                                                           \
-    const int b = L - 10 + 4, cnt = counts[b];                                                \
+    const int b = L - 10 + 4, cnt = num_counts_[b];                                           \
     if (cnt > 0) {                                                                            \
       const size_t smem = (size_t(1) << L) * (VB + 4) + (NT / 32) * SEG_SCRATCH_BYTES;        \
-      SG_CKE(set_smem(k_num_block<L, NT, MODE>, smem), "smem attr k_num_block");              \
-      E.prof_begin("k_num_block<" #L ">");                                                         \
-      k_num_block<L, NT, MODE><<<blocks_for(cnt, 1, (long long)sms * 8), NT, smem, stream>>>( \
+      SG_CK(smem_attr(k_num_block<L, NT, MODE>, smem), "smem attr k_num_block");              \
+      prof_begin("k_num_block<" #L ">");                                                       \
+      k_num_block<L, NT, MODE><<<blocks_for(cnt, 1, (long long)sms_ * 8), NT, smem, stream_>>>( \
           op, rows + (size_t)b * m, cnt, row_p, c_rowptr, c_col, c_val, status);              \
-      SG_LAUNCHED_E("k_num_block");                                                           \
+      SG_LAUNCHED("k_num_block");                                                             \
     }                                                                                         \
   }
   SG_NUM_BLOCK(10, 256) SG_NUM_BLOCK(11, 256) SG_NUM_BLOCK(12, 512) SG_NUM_BLOCK(13, 512)
 #undef SG_NUM_BLOCK
   return 0;
 }
+
+template int Engine::launch_numeric_mode<0>(int*, float*);
+template int Engine::launch_numeric_mode<1>(int*, float*);
 
 int Engine::multiply(const cm& A, const cm& B, cm* C_dev) {
   long long nnz = 0;

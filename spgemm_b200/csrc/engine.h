@@ -29,6 +29,7 @@ struct DevCounters {
   int sym_count[16];
   int num_count[16];
   int slice_count;
+  int mid_count;
   unsigned status;
   unsigned long long p_total;
   long long grand_total;
@@ -96,6 +97,8 @@ class Engine {
  private:
   int launch_symbolic_bins();
   int launch_numeric_bins(int* c_col, float* c_val);
+  template <int MODE> int launch_numeric_mode(int* c_col, float* c_val);
+  size_t big_dir_bytes() const;
   int scan_counts(const int* in, int n, long long* out);
   int check_status(unsigned st);
   template <class K> cudaError_t smem_attr(K kernel, size_t bytes);
@@ -115,7 +118,8 @@ class Engine {
   long long p_total_ = 0, nnz_c_ = 0;
   int sym_counts_[16] = {0};
   int num_counts_[16] = {0};
-  int nslices_ = 0;
+  int nslices_ = 0, nmid_ = 0;
+  long long big_capacity_ = 0;
   int n_long_sym_ = 0;
   int tn_run_slice_cap_ = 0;
   bool have_analysis_ = false;
@@ -123,7 +127,7 @@ class Engine {
 
   DevBuf a_rowptr_, a_col_, a_val_, cursor_, aoff_;
   DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
-  DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_;
+  DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_, mid_slices_, row_span_;
   DevBuf counters_, restrict_scratch_, bitmaps_;
   int bitmap_words_ = 0;  // per long row; 0 when the bitmaps are not kept
   int max_row_len_ = 0;

@@ -46,8 +46,9 @@ constexpr int SB_COUNT = 9;
 constexpr int SB_LONG = 8;
 // Numeric bins: 0..3 warp-per-row (2^6..2^9 slots), 4..7 block-per-row
 // (2^10..2^13 slots), 8 long rows (column slices).
-constexpr int NB_COUNT = 9;
+constexpr int NB_COUNT = 10;
 constexpr int NB_LONG = 8;
+constexpr int NB_MID = 9;  // mid rows in bitmap slices (counted here for statistics)
 
 constexpr int CHUNK_COLS = 2048;               // column granularity of slicing
 constexpr int CHUNK_WORDS = CHUNK_COLS / 32;
@@ -62,6 +63,8 @@ struct Tuning {
   int slice_cols;       // max columns of one numeric long slice (multiple of 2048)
   int sym_window;       // columns per symbolic bitmap window (multiple of 2048)
   int keep_bitmaps;     // keep long rows' symbolic bitmaps for the numeric pass
+  int mid_o_min;        // numeric: bitmap slice for rows with nnz_i > this ...
+  int mid_cols;         // ... whose column span is at most this many columns
 };
 
 __host__ __device__ inline int ceil_log2_ll(long long v) {
@@ -91,12 +94,15 @@ __host__ __device__ inline int num_bin_of(int o, long long p, const Tuning& t) {
   return lg - 10 + 4;  // lg <= 13 because o <= long_o_num <= 4096
 }
 
-// One column slice of a long row for the numeric pass.
+// One column slice of a row for the numeric bitmap kernel.
+constexpr int SLICE_WHOLE = 1;      // the slice holds all of the row's outputs
+constexpr int SLICE_BITS_KEPT = 2;  // the symbolic pass kept the row's bitmap
 struct Slice {
   long long out;  // first output position in C
   int row;
   int lo, hi;     // columns [lo, hi)
   int cnt;        // outputs in the slice
+  int flags;
 };
 
 // ---------------------------------------------------------------------------

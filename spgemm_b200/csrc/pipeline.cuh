@@ -93,7 +93,8 @@ __global__ void __launch_bounds__(RA_THREADS)
 k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_p,
                int* __restrict__ c_cnt, int* __restrict__ sym_count,
                int* __restrict__ sym_rows, unsigned long long* __restrict__ p_total,
-               int* __restrict__ max_row_len, unsigned* status, Tuning tn) {
+               int* __restrict__ max_row_len, int2* __restrict__ row_span, unsigned* status,
+               Tuning tn) {
   __shared__ int hist[SB_COUNT], base[SB_COUNT];
   __shared__ int rowbin[RA_ROWS], rowrank[RA_ROWS];
   __shared__ unsigned long long block_p;
@@ -110,19 +111,34 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
     }
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     long long acc = 0;
+    int lo = 0x7fffffff, hi = -1;  // column span of the row's products
     for (int b = rs; b < re; b += 32) {
       const int j = b + lane;
       long long len = 0;
       if (j < re) {
         const int k = op.a_col[j];
-        if ((unsigned)k < (unsigned)op.kdim) len = op.b_rowptr[k + 1] - op.b_rowptr[k];
-        else atomicOr(status, ST_BAD_INDEX);
+        if ((unsigned)k < (unsigned)op.kdim) {
+          const int bs = op.b_rowptr[k], be = op.b_rowptr[k + 1];
+          len = be - bs;
+          if (be > bs) {
+            lo = min(lo, op.b_col[bs]);
+            hi = max(hi, op.b_col[be - 1]);
+          }
+        } else {
+          atomicOr(status, ST_BAD_INDEX);
+        }
       }
       const long long incl = warp_incl_scan64(len);
       if (j < re) aoff[j] = (int)(acc + incl - len);
       acc += __shfl_sync(FULL, incl, 31);
     }
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      lo = min(lo, __shfl_xor_sync(FULL, lo, d));
+      hi = max(hi, __shfl_xor_sync(FULL, hi, d));
+    }
     if (lane == 0) {
+      row_span[i] = acc > 0 ? make_int2(lo, hi) : make_int2(0, -1);
       if (re - rs > 0) atomicMax(max_row_len, re - rs);
       row_p[i] = acc;
       if (acc >= (1ll << 31)) atomicOr(status, ST_ROW_TOO_LONG);
@@ -381,30 +397,50 @@ __global__ void k_rowptr_i64_to_i32_shift(const long long* __restrict__ in, int 
 
 constexpr int NBIN_THREADS = 256;
 
+__device__ __forceinline__ void push_slice(Slice* list, int* count, int capacity, const Slice& v,
+                                           unsigned* status) {
+  const int s = atomicAdd(count, 1);
+  if (s < capacity) list[s] = v;
+  else atomicOr(status, ST_SLICE_OVERFLOW);
+}
+
+// Numeric binning. Rows whose outputs fit one block's shared memory and whose
+// column span is narrow enough get one bitmap slice covering the span:
+// "long" rows (nnz_i > long_o_num) in the big-slice list, "mid" rows
+// (mid_o_min < nnz_i <= long_o_num) in the mid-slice list. Long rows that do
+// not fit are cut into column slices from the symbolic pass's per-chunk
+// counts. The rest go to the hash bins. `bits_kept`: the symbolic pass kept
+// the bitmaps of its long rows (P_i > long_p_sym).
 __global__ void __launch_bounds__(NBIN_THREADS)
 k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restrict__ row_p,
-          const long long* __restrict__ c_rowptr, int* __restrict__ num_count,
-          int* __restrict__ num_rows, const int* __restrict__ long_slot,
-          const int* __restrict__ chunk_cnt, int n_chunks, Slice* __restrict__ slices,
-          int* __restrict__ slice_count, int slice_capacity, unsigned* status, Tuning tn) {
+          const long long* __restrict__ c_rowptr, const int2* __restrict__ row_span,
+          int* __restrict__ num_count, int* __restrict__ num_rows,
+          const int* __restrict__ chunk_cnt, int n_chunks, const int* __restrict__ long_slot,
+          Slice* __restrict__ big, int* __restrict__ big_count, int big_capacity,
+          Slice* __restrict__ mid, int* __restrict__ mid_count, int bits_kept,
+          unsigned* status, Tuning tn) {
   __shared__ int hist[NB_COUNT], base[NB_COUNT];
   const int i = blockIdx.x * NBIN_THREADS + threadIdx.x;
   if (threadIdx.x < NB_COUNT) hist[threadIdx.x] = 0;
   __syncthreads();
   int bin = -1, rank = 0;
-  bool listed = false;  // long rows go to the slice list, not a row list
+  bool listed = false;  // bitmap rows go to a slice list, not a row list
   if (i < m) {
     const int o = c_cnt[i];
-    bin = num_bin_of(o, row_p[i], tn);
+    const long long p = row_p[i];
+    bin = num_bin_of(o, p, tn);
+    const int2 sp = row_span[i];
+    const int lo = sp.x & ~31;  // word aligned (saved bitmaps are indexed from column 0)
+    const int span = sp.y + 1 - lo;
+    const long long out0 = c_rowptr[i];
+    const int flags = SLICE_WHOLE | ((bits_kept && p > tn.long_p_sym) ? SLICE_BITS_KEPT : 0);
     if (bin == NB_LONG) {
       atomicAdd(&hist[NB_LONG], 1);
-      const long long out0 = c_rowptr[i];
-      if (o <= tn.slice_cap && n <= tn.slice_cols) {
-        const int s = atomicAdd(slice_count, 1);
-        if (s < slice_capacity) slices[s] = Slice{out0, i, 0, n, o};
-        else atomicOr(status, ST_SLICE_OVERFLOW);
+      if (o <= tn.slice_cap && span <= tn.slice_cols) {
+        push_slice(big, big_count, big_capacity, Slice{out0, i, lo, sp.y + 1, o, flags}, status);
       } else {
         const int* cc = chunk_cnt + (size_t)long_slot[i] * n_chunks;
+        const int sflags = flags & SLICE_BITS_KEPT;
         int lo_c = 0, acc = 0;
         long long out = out0;
         for (int c = 0; c < n_chunks; ++c) {
@@ -412,23 +448,22 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
           const bool too_many = acc + v > tn.slice_cap;
           const bool too_wide = (c + 1 - lo_c) * CHUNK_COLS > tn.slice_cols;
           if ((too_many || too_wide) && c > lo_c) {
-            if (acc) {
-              const int s = atomicAdd(slice_count, 1);
-              if (s < slice_capacity) slices[s] = Slice{out, i, lo_c * CHUNK_COLS, c * CHUNK_COLS, acc};
-              else atomicOr(status, ST_SLICE_OVERFLOW);
-            }
+            if (acc)
+              push_slice(big, big_count, big_capacity,
+                         Slice{out, i, lo_c * CHUNK_COLS, c * CHUNK_COLS, acc, sflags}, status);
             out += acc;
             lo_c = c;
             acc = 0;
           }
           acc += v;
         }
-        if (acc) {
-          const int s = atomicAdd(slice_count, 1);
-          if (s < slice_capacity) slices[s] = Slice{out, i, lo_c * CHUNK_COLS, n, acc};
-          else atomicOr(status, ST_SLICE_OVERFLOW);
-        }
+        if (acc)
+          push_slice(big, big_count, big_capacity, Slice{out, i, lo_c * CHUNK_COLS, n, acc, sflags},
+                     status);
       }
+    } else if (bin >= 0 && o > tn.mid_o_min && span <= tn.mid_cols) {
+      atomicAdd(&hist[NB_MID], 1);
+      push_slice(mid, mid_count, m, Slice{out0, i, lo, sp.y + 1, o, flags}, status);
     } else if (bin >= 0) {
       rank = atomicAdd(&hist[bin], 1);
       listed = true;
@@ -542,26 +577,41 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 }
 
 // ---------------------------------------------------------------------------
-// Numeric pass: long rows, one block per column slice
+// Numeric pass: bitmap slices (long and mid rows), one block per slice
 // ---------------------------------------------------------------------------
 
+// k-th (0-based) set bit of x (x has more than k set bits).
+__device__ __forceinline__ int nth_set_bit(unsigned x, int k) {
+  int pos = 0;
+#pragma unroll
+  for (int sh = 16; sh > 0; sh >>= 1) {
+    const unsigned low = x & ((1u << sh) - 1u);
+    const int c = __popc(low);
+    if (k >= c) { k -= c; x >>= sh; pos += sh; }
+    else { x = low; }
+  }
+  return pos;
+}
+
 // Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap].
-// Pass 1 sets presence bits, a block scan turns popcounts into ranks, pass 2
-// adds every product into the slot given by its column's rank, and the slice
-// is written out in column order straight from the bitmap.
-template <int MODE>
-__global__ void __launch_bounds__(LONG_THREADS)
+// The presence bits come from the symbolic pass when it kept them, else from
+// a first expansion pass; a block scan turns popcounts into ranks; the value
+// pass adds every product into the slot given by its column's rank (a
+// counting sort on the column, so the slice comes out in column order); the
+// write-out walks the bitmap 32 words per warp with coalesced stores.
+template <int MODE, int NT>
+__global__ void __launch_bounds__(NT)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            const long long* __restrict__ row_p, int dir_words, int cap,
            int* __restrict__ scratch, int scratch_stride,
            const unsigned* __restrict__ bitmaps, int bitmap_words,
            const int* __restrict__ long_slot,
            int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
-  constexpr int NW = LONG_THREADS / 32;
+  constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long scan_shm[33];
   __shared__ int carry_shm;
-  const int warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
   unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
@@ -571,23 +621,23 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     const int i = sl.row;
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     int* roff = seg_start + (re - rs);
-    const bool full = sl.lo == 0 && sl.hi == op.n;
+    const bool whole = (sl.flags & SLICE_WHOLE) != 0;
     const int nw = (sl.hi - sl.lo + 31) >> 5;
     const int cnt = sl.cnt;
     if (nw > dir_words || cnt > cap) {  // host sizing guarantees this never trips
       if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
       continue;
     }
-    const bool have_bits = bitmap_words > 0;
+    const bool have_bits = bitmap_words > 0 && (sl.flags & SLICE_BITS_KEPT);
     if (have_bits) {  // the symbolic pass kept this row's presence bitmap
       const unsigned* src = bitmaps + (size_t)long_slot[i] * bitmap_words + (sl.lo >> 5);
-      for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(__ldg(src + t), 0u);
+      for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(__ldg(src + t), 0u);
     } else {
-      for (int t = threadIdx.x; t < nw; t += LONG_THREADS) dir[t] = make_uint2(0u, 0u);
+      for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(0u, 0u);
     }
     // products of the slice: the whole row, or its restriction to [lo, hi)
     int p;
-    if (full) {
+    if (whole) {
       p = (int)row_p[i];
       __syncthreads();
     } else {
@@ -598,7 +648,7 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     if (!have_bits) {
       LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (full) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        if (whole) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
       __syncthreads();
@@ -606,7 +656,7 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     // ranks: exclusive scan of popcounts over the nw directory words
     long long tot;
     {
-      const int per = (nw + LONG_THREADS - 1) / LONG_THREADS;
+      const int per = (nw + NT - 1) / NT;
       const int w0 = threadIdx.x * per;
       int local = 0;
       for (int q = 0; q < per; ++q)
@@ -622,39 +672,68 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     }
     if (MODE == 0) {
       float* vals = reinterpret_cast<float*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += LONG_THREADS) vals[t] = 0.f;
+      for (int t = threadIdx.x; t < cnt; t += NT) vals[t] = 0.f;
     } else {
       double* vals = reinterpret_cast<double*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += LONG_THREADS) vals[t] = 0.0;
+      for (int t = threadIdx.x; t < cnt; t += NT) vals[t] = 0.0;
     }
     __syncthreads();
-    // pass 2: values
+    // value pass
     if (MODE == 0) {
       LongValPlain f{dir, reinterpret_cast<float*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (full) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     } else {
       LongValF64 f{dir, reinterpret_cast<double*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (full) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     }
     __syncthreads();
-    // write out in column order
-    for (int w = threadIdx.x; w < nw; w += LONG_THREADS) {
-      unsigned bitsw = dir[w].x;
-      int rnk = (int)dir[w].y;
-      while (bitsw) {
-        const int b = __ffs(bitsw) - 1;
-        bitsw &= bitsw - 1u;
-        const long long o = sl.out + rnk;
-        c_col[o] = sl.lo + w * 32 + b;
-        if (MODE == 0) c_val[o] = reinterpret_cast<float*>(vbase)[rnk];
-        else c_val[o] = finalize_value(reinterpret_cast<double*>(vbase)[rnk]);
-        ++rnk;
+    // write-out: each warp emits the outputs of 32 consecutive words in
+    // windows of 32 consecutive output positions
+    for (int g = warp; g * 32 < nw; g += NW) {
+      const int w = g * 32 + lane;
+      unsigned bits = w < nw ? dir[w].x : 0u;
+      int pc = __popc(bits);
+      const int gbase = (int)dir[g * 32].y;
+      // compact the non-empty words (word index travels in `len`'s place)
+      int word = w;
+      float unused = 0.f;
+      const unsigned ne = __ballot_sync(FULL, pc > 0);
+      const int nne = __popc(ne);
+      if (ne != (nne == 32 ? FULL : ((1u << nne) - 1u))) {
+        const int rk = __popc(ne & ((1u << lane) - 1u));
+        if (pc > 0) { sc->bstart[rk] = (int)bits; sc->len[rk] = word; }
+        __syncwarp();
+        if (lane < nne) { bits = (unsigned)sc->bstart[lane]; word = sc->len[lane]; pc = __popc(bits); }
+        else { bits = 0u; pc = 0; }
+        __syncwarp();
+      }
+      (void)unused;
+      const int incl = warp_incl_scan(pc);
+      const int total = __shfl_sync(FULL, incl, 31);
+      const int st = incl - pc;
+      int nbefore = 0;
+      for (int b0 = 0; b0 < total; b0 += 32) {
+        const unsigned bit = (pc > 0 && st >= b0 && st < b0 + 32) ? (1u << (st - b0)) : 0u;
+        const unsigned starts = __reduce_or_sync(FULL, bit);
+        const int owner = nbefore + __popc(starts & (FULL >> (31 - lane))) - 1;
+        nbefore += __popc(starts);
+        const unsigned obits = __shfl_sync(FULL, bits, owner);
+        const int oword = __shfl_sync(FULL, word, owner);
+        const int ost = __shfl_sync(FULL, st, owner);
+        const int q = b0 + lane;
+        if (q < total) {
+          const int r = gbase + q;
+          const long long o = sl.out + r;
+          c_col[o] = sl.lo + oword * 32 + nth_set_bit(obits, q - ost);
+          if (MODE == 0) c_val[o] = reinterpret_cast<float*>(vbase)[r];
+          else c_val[o] = finalize_value(reinterpret_cast<double*>(vbase)[r]);
+        }
       }
     }
     __syncthreads();

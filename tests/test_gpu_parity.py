@@ -158,6 +158,8 @@ TUNINGS = [
     dict(long_p_sym=256, long_o_num=256),                   # mid rows take the long path
     dict(sym_window=4096, slice_cols=4096, slice_cap=2048,  # multi-window symbolic pass,
          keep_bitmaps=0),                                   # restricted numeric slices
+    dict(mid_o_min=0),                                      # every row with outputs: bitmap kernel
+    dict(mid_cols=0),                                       # no mid bitmap rows: hash bins only
 ]
 
 
