@@ -311,7 +311,8 @@ int Engine::analyze(const cm& A, const cm& B) {
   SG_CK(row_p_.ensure(sizeof(long long) * (size_t)std::max(m, 1)), "alloc row_p");
   SG_CK(sym_rows_.ensure(sizeof(int) * (size_t)SB_COUNT * std::max(m, 1)), "alloc sym_rows");
   SG_CK(row_span_.ensure(sizeof(int2) * (size_t)std::max(m, 1)), "alloc row spans");
-  op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_};
+  const int vec_ok = ((reinterpret_cast<uintptr_t>(B.idx) | reinterpret_cast<uintptr_t>(B.val)) & 15) == 0;
+  op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_, vec_ok};
   if (m > 0) {
     prof_begin("k_row_analysis");
     k_row_analysis<<<(m + RA_ROWS - 1) / RA_ROWS, RA_THREADS, 0, stream_>>>(

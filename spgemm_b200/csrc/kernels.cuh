@@ -38,6 +38,7 @@ struct Operands {
   const int* __restrict__ b_col;
   const float* __restrict__ b_val;
   int m, kdim, n;
+  int vec_ok;  // b_col and b_val are 16-byte aligned: 128-bit loads allowed
 };
 
 // Symbolic bins: 0..4 warp-per-row hash (2^6..2^10 slots), 5..7 block-per-row
@@ -192,6 +193,81 @@ __device__ __forceinline__ void run_segments(int cnt, int bstart, int len, float
   }
 }
 
+// Segments at least this long are walked by the whole warp with 128-bit
+// loads (4 products per lane per step) instead of the flattened walk.
+constexpr int VEC_MIN_SEG = 128;
+
+// One segment B positions [bs, bs + len) scaled by a, whole warp: scalar head
+// up to the first 16-byte boundary, int4/float4 body, scalar tail.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_run_segment_vec(int bs, int len, float a,
+                                                     const int* __restrict__ b_col,
+                                                     const float* __restrict__ b_val, F& f) {
+  const int lane = lane_id();
+  const int end = bs + len;
+  const int head = min((4 - (bs & 3)) & 3, len);
+  if (lane < head) {
+    const int pos = bs + lane;
+    f(__ldg(b_col + pos), a, NEED_VAL ? __ldg(b_val + pos) : 0.f);
+  }
+  const int body0 = bs + head;
+  const int n4 = (end - body0) >> 2;
+  const int4* c4 = reinterpret_cast<const int4*>(b_col + body0);
+  const float4* v4 = reinterpret_cast<const float4*>(b_val + body0);
+  constexpr int VU = 4;  // groups of 4 products whose loads are in flight together
+  int g = lane;
+  for (; g + 32 * (VU - 1) < n4; g += 32 * VU) {
+    int4 c[VU];
+    float4 v[VU];
+#pragma unroll
+    for (int u = 0; u < VU; ++u) {
+      c[u] = __ldg(c4 + g + 32 * u);
+      v[u] = NEED_VAL ? __ldg(v4 + g + 32 * u) : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < VU; ++u) {
+      f(c[u].x, a, v[u].x);
+      f(c[u].y, a, v[u].y);
+      f(c[u].z, a, v[u].z);
+      f(c[u].w, a, v[u].w);
+    }
+  }
+  for (; g < n4; g += 32) {
+    const int4 c = __ldg(c4 + g);
+    const float4 v = NEED_VAL ? __ldg(v4 + g) : make_float4(0.f, 0.f, 0.f, 0.f);
+    f(c.x, a, v.x);
+    f(c.y, a, v.y);
+    f(c.z, a, v.z);
+    f(c.w, a, v.w);
+  }
+  const int tail0 = body0 + 4 * n4;
+  if (tail0 + lane < end) {
+    const int pos = tail0 + lane;
+    f(__ldg(b_col + pos), a, NEED_VAL ? __ldg(b_val + pos) : 0.f);
+  }
+}
+
+// All products of the warp's (<= 32) segments: long ones one at a time with
+// the vector walk, the rest compacted and walked flattened.
+template <bool NEED_VAL, class F>
+__device__ __forceinline__ void warp_run_batch(const Operands& op, int bstart, int len, float a,
+                                               F& f, SegScratch* sc) {
+  if (op.vec_ok) {
+    unsigned big = __ballot_sync(FULL, len >= VEC_MIN_SEG);
+    while (big) {
+      const int src = __ffs(big) - 1;
+      big &= big - 1u;
+      const int sbs = __shfl_sync(FULL, bstart, src);
+      const int sl = __shfl_sync(FULL, len, src);
+      const float sa = __shfl_sync(FULL, a, src);
+      warp_run_segment_vec<NEED_VAL>(sbs, sl, sa, op.b_col, op.b_val, f);
+    }
+    if (len >= VEC_MIN_SEG) len = 0;
+  }
+  const int cnt = compact_segments(bstart, len, a, sc);
+  if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+}
+
 // Products per warp work unit when the warps of a block share one row of
 // `p` products. Units are equal slices of the row's flattened product
 // sequence, so one unit per warp is already balanced; each unit costs one
@@ -219,8 +295,7 @@ __device__ __forceinline__ void warp_expand_row(const Operands& op, int rs, int 
       bstart = __ldg(op.b_rowptr + k);
       len = __ldg(op.b_rowptr + k + 1) - bstart;
     }
-    const int cnt = compact_segments(bstart, len, a, sc);
-    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+    warp_run_batch<NEED_VAL>(op, bstart, len, a, f, sc);
   }
 }
 
@@ -259,8 +334,7 @@ __device__ __forceinline__ void warp_expand_range(const Operands& op, int rs, in
       }
     }
     const bool done = __any_sync(FULL, past);
-    const int cnt = compact_segments(bstart, len, a, sc);
-    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+    warp_run_batch<NEED_VAL>(op, bstart, len, a, f, sc);
     if (done) break;
   }
 }
@@ -350,8 +424,7 @@ __device__ __forceinline__ void warp_expand_explicit(const Operands& op, int rs,
       }
     }
     const bool done = __any_sync(FULL, past);
-    const int cnt = compact_segments(bstart, len, a, sc);
-    if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+    warp_run_batch<NEED_VAL>(op, bstart, len, a, f, sc);
     if (done) break;
   }
 }
@@ -381,8 +454,7 @@ __device__ __forceinline__ void warp_expand_restricted(const Operands& op, int j
       }
     }
   }
-  const int cnt = compact_segments(bstart, len, a, sc);
-  if (cnt) run_segments<NEED_VAL>(cnt, bstart, len, a, op.b_col, op.b_val, f);
+  warp_run_batch<NEED_VAL>(op, bstart, len, a, f, sc);
 }
 
 // ---------------------------------------------------------------------------

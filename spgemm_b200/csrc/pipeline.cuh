@@ -517,9 +517,9 @@ k_num_warp(Operands op, const int* __restrict__ rows, int nrows,
     if (lane == 0 && ((cnt < T && keys[cnt] != EMPTY_KEY) || keys[cnt - 1] == EMPTY_KEY))
       atomicOr(status, ST_COUNT_MISMATCH);
     for (int t = lane; t < cnt; t += 32) {
-      c_col[o + t] = (int)keys[t];
-      if (MODE == 0) c_val[o + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
-      else c_val[o + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+      __stcs(c_col + o + t, (int)keys[t]);
+      if (MODE == 0) __stcs(c_val + o + t, finalize_value(reinterpret_cast<float*>(vals)[t]));
+      else __stcs(c_val + o + t, finalize_value(reinterpret_cast<float2*>(vals)[t]));
     }
     __syncwarp();
   }
@@ -567,10 +567,10 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
         ((cnt < T && keys[cnt] != EMPTY_KEY) || keys[cnt - 1] == EMPTY_KEY))
       atomicOr(status, ST_COUNT_MISMATCH);
     for (int t = threadIdx.x; t < cnt; t += NT) {
-      c_col[o + t] = (int)keys[t];
-      if (MODE == 0) c_val[o + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
-      else if (fp64) c_val[o + t] = finalize_value(reinterpret_cast<double*>(vals)[t]);
-      else c_val[o + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+      __stcs(c_col + o + t, (int)keys[t]);
+      if (MODE == 0) __stcs(c_val + o + t, finalize_value(reinterpret_cast<float*>(vals)[t]));
+      else if (fp64) __stcs(c_val + o + t, finalize_value(reinterpret_cast<double*>(vals)[t]));
+      else __stcs(c_val + o + t, finalize_value(reinterpret_cast<float2*>(vals)[t]));
     }
     __syncthreads();
   }
@@ -580,25 +580,12 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 // Numeric pass: bitmap slices (long and mid rows), one block per slice
 // ---------------------------------------------------------------------------
 
-// k-th (0-based) set bit of x (x has more than k set bits).
-__device__ __forceinline__ int nth_set_bit(unsigned x, int k) {
-  int pos = 0;
-#pragma unroll
-  for (int sh = 16; sh > 0; sh >>= 1) {
-    const unsigned low = x & ((1u << sh) - 1u);
-    const int c = __popc(low);
-    if (k >= c) { k -= c; x >>= sh; pos += sh; }
-    else { x = low; }
-  }
-  return pos;
-}
-
 // Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap].
 // The presence bits come from the symbolic pass when it kept them, else from
 // a first expansion pass; a block scan turns popcounts into ranks; the value
 // pass adds every product into the slot given by its column's rank (a
 // counting sort on the column, so the slice comes out in column order); the
-// write-out walks the bitmap 32 words per warp with coalesced stores.
+// write-out copies the values in order and expands the bitmap into columns.
 template <int MODE, int NT>
 __global__ void __launch_bounds__(NT)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
@@ -611,7 +598,7 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long scan_shm[33];
   __shared__ int carry_shm;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
   unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
@@ -693,47 +680,22 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       }
     }
     __syncthreads();
-    // write-out: each warp emits the outputs of 32 consecutive words in
-    // windows of 32 consecutive output positions
-    for (int g = warp; g * 32 < nw; g += NW) {
-      const int w = g * 32 + lane;
-      unsigned bits = w < nw ? dir[w].x : 0u;
-      int pc = __popc(bits);
-      const int gbase = (int)dir[g * 32].y;
-      // compact the non-empty words (word index travels in `len`'s place)
-      int word = w;
-      float unused = 0.f;
-      const unsigned ne = __ballot_sync(FULL, pc > 0);
-      const int nne = __popc(ne);
-      if (ne != (nne == 32 ? FULL : ((1u << nne) - 1u))) {
-        const int rk = __popc(ne & ((1u << lane) - 1u));
-        if (pc > 0) { sc->bstart[rk] = (int)bits; sc->len[rk] = word; }
-        __syncwarp();
-        if (lane < nne) { bits = (unsigned)sc->bstart[lane]; word = sc->len[lane]; pc = __popc(bits); }
-        else { bits = 0u; pc = 0; }
-        __syncwarp();
-      }
-      (void)unused;
-      const int incl = warp_incl_scan(pc);
-      const int total = __shfl_sync(FULL, incl, 31);
-      const int st = incl - pc;
-      int nbefore = 0;
-      for (int b0 = 0; b0 < total; b0 += 32) {
-        const unsigned bit = (pc > 0 && st >= b0 && st < b0 + 32) ? (1u << (st - b0)) : 0u;
-        const unsigned starts = __reduce_or_sync(FULL, bit);
-        const int owner = nbefore + __popc(starts & (FULL >> (31 - lane))) - 1;
-        nbefore += __popc(starts);
-        const unsigned obits = __shfl_sync(FULL, bits, owner);
-        const int oword = __shfl_sync(FULL, word, owner);
-        const int ost = __shfl_sync(FULL, st, owner);
-        const int q = b0 + lane;
-        if (q < total) {
-          const int r = gbase + q;
-          const long long o = sl.out + r;
-          c_col[o] = sl.lo + oword * 32 + nth_set_bit(obits, q - ost);
-          if (MODE == 0) c_val[o] = reinterpret_cast<float*>(vbase)[r];
-          else c_val[o] = finalize_value(reinterpret_cast<double*>(vbase)[r]);
-        }
+    // write-out: values are already in output order (coalesced copy);
+    // columns are expanded word by word from the bitmap
+    if (MODE == 0) {
+      const float* vals = reinterpret_cast<const float*>(vbase);
+      for (int t = threadIdx.x; t < cnt; t += NT) __stcs(c_val + sl.out + t, vals[t]);
+    } else {
+      const double* vals = reinterpret_cast<const double*>(vbase);
+      for (int t = threadIdx.x; t < cnt; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
+    }
+    for (int w = threadIdx.x; w < nw; w += NT) {
+      unsigned bits = dir[w].x;
+      long long o = sl.out + dir[w].y;
+      const int cbase = sl.lo + w * 32;
+      while (bits) {
+        __stcs(c_col + o++, cbase + __ffs(bits) - 1);
+        bits &= bits - 1u;
       }
     }
     __syncthreads();

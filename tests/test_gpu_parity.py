@@ -187,3 +187,68 @@ def test_bad_tuning_rejected():
             h.set_tuning(slice_cols=1000)
         with pytest.raises(sg.SpgemmError):
             h.set_tuning(long_p_sym=5000)
+
+
+def _dev(a, dtype, offset=0):
+    """Device copy of a, starting `offset` elements into a larger buffer (to
+    misalign it on purpose)."""
+    import torch
+    t = torch.zeros(len(a) + offset + 1, dtype=dtype, device="cuda")
+    t[offset:offset + len(a)] = torch.from_numpy(np.ascontiguousarray(a)).to(dtype)
+    return t, t[offset:]
+
+
+@pytest.mark.parametrize("offset", [0, 1])
+def test_device_api_two_phase(offset):
+    """spgemm_symbolic + spgemm_numeric on device pointers into caller buffers;
+    offset 1 misaligns B's arrays so the 128-bit load path is disabled."""
+    import torch
+    A = W.rmat(13, 12, 7, values="sym")
+    Ac = A.to_csc()
+    keep = []
+    a_ptr = _dev(Ac.colptr, torch.int32)[1]; a_idx = _dev(Ac.rowidx, torch.int32)[1]
+    a_val = _dev(Ac.val, torch.float32)[1]
+    b_ptr = _dev(A.rowptr, torch.int32)[1]
+    b_idx_base, b_idx = _dev(A.col, torch.int32, offset)
+    b_val_base, b_val = _dev(A.val, torch.float32, offset)
+    keep += [b_idx_base, b_val_base]
+    Acm = sg.device_cm(a_ptr.data_ptr(), a_idx.data_ptr(), a_val.data_ptr(), A.nnz, A.rows, A.cols, sg.COL_MAJOR)
+    Bcm = sg.device_cm(b_ptr.data_ptr(), b_idx.data_ptr(), b_val.data_ptr(), A.nnz, A.rows, A.cols, sg.ROW_MAJOR)
+    with sg.Handle() as h:
+        h.set_stream(torch.cuda.current_stream().cuda_stream)
+        nnz = h.symbolic(Acm, Bcm)
+        rp = torch.empty(A.rows + 1, dtype=torch.int32, device="cuda")
+        col = torch.empty(nnz, dtype=torch.int32, device="cuda")
+        val = torch.empty(nnz, dtype=torch.float32, device="cuda")
+        h.numeric(rp.data_ptr(), col.data_ptr(), val.data_ptr())
+        torch.cuda.synchronize()
+    ref = ref_product(A, A)
+    assert_structure_equal(rp.cpu().numpy(), col.cpu().numpy(), ref["rowptr"], ref["col"])
+    assert_values_close(val.cpu().numpy(), ref, plain_tolerance(ref))
+
+
+def test_numeric_before_symbolic_is_an_error():
+    with sg.Handle() as h:
+        with pytest.raises(sg.SpgemmError) as e:
+            h.numeric(0, 0, 0)
+        assert e.value.status == 5
+
+
+def test_invalid_inputs_rejected():
+    A = W.er(100, 4.0, 1)
+    bad = W.Csr(A.rows, A.cols, A.rowptr.copy(), A.col.copy(), A.val.copy())
+    bad.col[3] = A.cols + 5            # column out of range
+    with sg.Handle() as h:
+        with pytest.raises(sg.SpgemmError) as e:
+            h.multiply_host(A.to_csc(), bad)
+        assert e.value.status == 1
+        uns = W.Csr(A.rows, A.cols, A.rowptr.copy(), A.col.copy(), A.val.copy())
+        r = int(np.argmax(np.diff(A.rowptr) >= 2))
+        s = A.rowptr[r]
+        uns.col[s], uns.col[s + 1] = A.col[s + 1], A.col[s]   # unsorted B row
+        with pytest.raises(sg.SpgemmError):
+            h.multiply_host(A.to_csc(), uns)
+        # the handle stays usable after rejected inputs
+        C = h.multiply_host(A.to_csc(), A)
+        ref = ref_product(A, A)
+        assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
