@@ -503,11 +503,11 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     const int dir_words = (int)(big_dir_bytes() / sizeof(uint2));
     const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes() +
                         (size_t)tn_run_slice_cap_ * (MODE ? 8 : 4);
-    SG_CK(smem_attr(k_num_long<MODE, LONG_THREADS>, smem), "smem attr k_num_long");
+    SG_CK(smem_attr(k_num_long<MODE, LONG_THREADS, false>, smem), "smem attr k_num_long");
     const int grid = blocks_for(nslices_, 1, (long long)sms_ * 2);
     SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
     prof_begin("k_num_long");
-    k_num_long<MODE, LONG_THREADS><<<grid, LONG_THREADS, smem, stream_>>>(
+    k_num_long<MODE, LONG_THREADS, false><<<grid, LONG_THREADS, smem, stream_>>>(
         op, slices_buf_.as<Slice>(), nslices_, row_p, dir_words, tn_run_slice_cap_,
         restrict_scratch_.as<int>(), stride, bitmaps_.as<unsigned>(), bitmap_words_,
         long_slot_.as<int>(), c_col, c_val, status);
@@ -516,14 +516,16 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   // mid bitmap slices: whole rows of at most long_o_num outputs, 512 threads
   if (nmid_ > 0) {
     const int width = std::min(n_, tn_.mid_cols) + 32;  // + alignment of lo down to 32
-    const int dir_words = (width + 31) / 32;
+    const int dir_words = (width + 31) / 32;            // <= 8193, so l1 fits 512 threads
+    const int cap = tn_.long_o_num;
     const size_t smem = (MID_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)dir_words * sizeof(uint2) +
-                        (size_t)tn_.long_o_num * (MODE ? 8 : 4);
-    SG_CK(smem_attr(k_num_long<MODE, MID_THREADS>, smem), "smem attr k_num_long mid");
+                        (size_t)cap * (MODE ? 8 : 4) + sizeof(unsigned) * ((dir_words + 31) / 32) +
+                        sizeof(int) * (size_t)cap;
+    SG_CK(smem_attr(k_num_long<MODE, MID_THREADS, true>, smem), "smem attr k_num_long mid");
     const int grid = blocks_for(nmid_, 1, (long long)sms_ * 4);
     prof_begin("k_num_mid");
-    k_num_long<MODE, MID_THREADS><<<grid, MID_THREADS, smem, stream_>>>(
-        op, mid_slices_.as<Slice>(), nmid_, row_p, dir_words, tn_.long_o_num,
+    k_num_long<MODE, MID_THREADS, true><<<grid, MID_THREADS, smem, stream_>>>(
+        op, mid_slices_.as<Slice>(), nmid_, row_p, dir_words, cap,
         restrict_scratch_.as<int>(), 0, bitmaps_.as<unsigned>(), bitmap_words_,
         long_slot_.as<int>(), c_col, c_val, status);
     SG_LAUNCHED("k_num_mid");

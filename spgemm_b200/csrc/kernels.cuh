@@ -574,6 +574,26 @@ struct LongBits {
   }
 };
 
+// LongBits that also records, in a second-level bitmap l1 (one bit per
+// directory word), which directory words became non-empty.
+struct LongBitsTracked {
+  uint2* dir;
+  unsigned* l1;
+  int lo;
+  unsigned width;
+  unsigned* status;
+  __device__ __forceinline__ void operator()(int col, float, float) {
+    const unsigned c = (unsigned)(col - lo);
+    if (c < width) {
+      const unsigned w = c >> 5;
+      const unsigned old = atomicOr(&dir[w].x, 1u << (c & 31));
+      if (old == 0u) atomicOr(l1 + (w >> 5), 1u << (w & 31));
+    } else {
+      atomicOr(status, ST_BAD_INDEX);
+    }
+  }
+};
+
 // Output slot of `col` (only columns whose bit pass 1 set reach here, so
 // the slot is below the slice's output count).
 __device__ __forceinline__ int long_slot(const uint2* dir, int lo, int col) {

@@ -580,13 +580,20 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 // Numeric pass: bitmap slices (long and mid rows), one block per slice
 // ---------------------------------------------------------------------------
 
-// Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap].
+// Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap]
+// (| sparse mode: l1 bits[dir_words/32 + 1] | touched word list[cap]).
 // The presence bits come from the symbolic pass when it kept them, else from
 // a first expansion pass; a block scan turns popcounts into ranks; the value
 // pass adds every product into the slot given by its column's rank (a
 // counting sort on the column, so the slice comes out in column order); the
 // write-out copies the values in order and expands the bitmap into columns.
-template <int MODE, int NT>
+//
+// SPARSE (used for mid rows, at most `cap` outputs over up to 2^18 columns):
+// the directory is cleared once per block and kept clean between slices;
+// ranks, write-out and cleanup visit only the directory words that became
+// non-empty (tracked in l1), so a slice costs O(products + outputs) instead
+// of O(span / 32).
+template <int MODE, int NT, bool SPARSE>
 __global__ void __launch_bounds__(NT)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            const long long* __restrict__ row_p, int dir_words, int cap,
@@ -602,7 +609,14 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
   unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
+  const int l1_words = (dir_words + 31) >> 5;
+  unsigned* l1 = reinterpret_cast<unsigned*>(vbase + (size_t)cap * (MODE ? 8 : 4));
+  int* touched = reinterpret_cast<int*>(l1 + l1_words);
   int* seg_start = scratch + (size_t)blockIdx.x * scratch_stride;
+  if (SPARSE) {
+    for (int t = threadIdx.x; t < dir_words; t += NT) dir[t] = make_uint2(0u, 0u);
+    for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
+  }
   for (int s = blockIdx.x; s < nslices; s += gridDim.x) {
     const Slice sl = slices[s];
     const int i = sl.row;
@@ -611,15 +625,26 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     const bool whole = (sl.flags & SLICE_WHOLE) != 0;
     const int nw = (sl.hi - sl.lo + 31) >> 5;
     const int cnt = sl.cnt;
-    if (nw > dir_words || cnt > cap) {  // host sizing guarantees this never trips
+    if (nw > dir_words || cnt > cap || (SPARSE && !whole)) {  // host sizing prevents this
       if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
       continue;
     }
     const bool have_bits = bitmap_words > 0 && (sl.flags & SLICE_BITS_KEPT);
     if (have_bits) {  // the symbolic pass kept this row's presence bitmap
       const unsigned* src = bitmaps + (size_t)long_slot[i] * bitmap_words + (sl.lo >> 5);
-      for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(__ldg(src + t), 0u);
-    } else {
+      if (SPARSE) {
+        __syncthreads();  // previous slice's cleanup is complete
+        for (int t = threadIdx.x; t < nw; t += NT) {
+          const unsigned b = __ldg(src + t);
+          if (b) {
+            dir[t].x = b;
+            atomicOr(l1 + (t >> 5), 1u << (t & 31));
+          }
+        }
+      } else {
+        for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(__ldg(src + t), 0u);
+      }
+    } else if (!SPARSE) {
       for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(0u, 0u);
     }
     // products of the slice: the whole row, or its restriction to [lo, hi)
@@ -633,16 +658,47 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     const int U = chunk_for(p, NW, 1 << 20);
     // pass 1: presence bits (only when the bitmap was not kept)
     if (!have_bits) {
-      LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (whole) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
-        else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
+      if (SPARSE) {
+        LongBitsTracked f{dir, l1, sl.lo, (unsigned)(sl.hi - sl.lo), status};
+        for (int c0 = warp * U; c0 < p; c0 += NW * U)
+          warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+      } else {
+        LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
+        for (int c0 = warp * U; c0 < p; c0 += NW * U) {
+          if (whole) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+          else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
+        }
       }
       __syncthreads();
     }
-    // ranks: exclusive scan of popcounts over the nw directory words
+    // ranks: exclusive scan of popcounts over the directory words
     long long tot;
-    {
+    int nt = 0;  // sparse: number of touched words
+    if (SPARSE) {
+      // touched word list, in column order, from l1
+      const int nl1 = (nw + 31) >> 5;
+      long long l1tot;
+      const unsigned myl1 = threadIdx.x < nl1 ? l1[threadIdx.x] : 0u;  // nl1 <= NT (host)
+      long long pos = block_excl_scan64(__popc(myl1), scan_shm, l1tot);
+      for (unsigned b = myl1; b; b &= b - 1u) {
+        if (pos < cap) touched[pos] = threadIdx.x * 32 + __ffs(b) - 1;  // list holds cap words
+        ++pos;
+      }
+      nt = (int)min(l1tot, (long long)cap);  // more than cap touched words: count mismatch below
+      __syncthreads();
+      const int per = (nt + NT - 1) / NT;
+      const int t0 = threadIdx.x * per;
+      int local = 0;
+      for (int q = 0; q < per; ++q)
+        if (t0 + q < nt) local += __popc(dir[touched[t0 + q]].x);
+      long long run = block_excl_scan64(local, scan_shm, tot);
+      for (int q = 0; q < per; ++q)
+        if (t0 + q < nt) {
+          uint2& d = dir[touched[t0 + q]];
+          d.y = (unsigned)run;
+          run += __popc(d.x);
+        }
+    } else {
       const int per = (nw + NT - 1) / NT;
       const int w0 = threadIdx.x * per;
       int local = 0;
@@ -652,9 +708,14 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       for (int q = 0; q < per; ++q)
         if (w0 + q < nw) { dir[w0 + q].y = (unsigned)run; run += __popc(dir[w0 + q].x); }
     }
-    if (tot != cnt) {  // block-uniform: slots would not fit the slice
+    if (tot != cnt || (SPARSE && nt == cap && cnt < cap)) {  // block-uniform
       if (threadIdx.x == 0) atomicOr(status, ST_COUNT_MISMATCH);
       __syncthreads();
+      if (SPARSE) {  // restore the clean directory before the next slice
+        for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(0u, 0u);
+        for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
+        __syncthreads();
+      }
       continue;
     }
     if (MODE == 0) {
@@ -689,13 +750,30 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       const double* vals = reinterpret_cast<const double*>(vbase);
       for (int t = threadIdx.x; t < cnt; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
     }
-    for (int w = threadIdx.x; w < nw; w += NT) {
-      unsigned bits = dir[w].x;
-      long long o = sl.out + dir[w].y;
-      const int cbase = sl.lo + w * 32;
-      while (bits) {
-        __stcs(c_col + o++, cbase + __ffs(bits) - 1);
-        bits &= bits - 1u;
+    if (SPARSE) {
+      for (int t = threadIdx.x; t < nt; t += NT) {
+        const int w = touched[t];
+        unsigned bits = dir[w].x;
+        long long o = sl.out + dir[w].y;
+        const int cbase = sl.lo + w * 32;
+        while (bits) {
+          __stcs(c_col + o++, cbase + __ffs(bits) - 1);
+          bits &= bits - 1u;
+        }
+      }
+      __syncthreads();
+      // leave the directory clean for the next slice
+      for (int t = threadIdx.x; t < nt; t += NT) dir[touched[t]] = make_uint2(0u, 0u);
+      for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
+    } else {
+      for (int w = threadIdx.x; w < nw; w += NT) {
+        unsigned bits = dir[w].x;
+        long long o = sl.out + dir[w].y;
+        const int cbase = sl.lo + w * 32;
+        while (bits) {
+          __stcs(c_col + o++, cbase + __ffs(bits) - 1);
+          bits &= bits - 1u;
+        }
       }
     }
     __syncthreads();
