@@ -1,0 +1,77 @@
+"""The reference's mm.h call protocol end to end: a C driver equivalent to the
+reference's src/main.cu, compiled against include/ and the library, run on a
+Matrix-Market file. Its printed P and nnzC, and the C it writes, are checked
+against the oracle (values are sums of 1.1 * 1.1: the reader forces 1.1)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+import spgemm_b200 as sg
+from spgemm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+ROOT = Path(__file__).resolve().parents[1]
+
+
+@pytest.fixture(scope="module")
+def outer_bin(tmp_path_factory):
+    d = tmp_path_factory.mktemp("outer")
+    exe = d / "outer"
+    libdir = sg.LIB_PATH.parent
+    subprocess.run(["gcc", "-O2", f"-I{ROOT / 'include'}", str(ROOT / "spgemm_b200/examples/outer.c"),
+                    f"-L{libdir}", "-lspgemm_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    return exe
+
+
+def write_mtx(path, M: W.Csr):
+    r = np.repeat(np.arange(M.rows), np.diff(M.rowptr))
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real general\n")
+        f.write(f"{M.cols} {M.rows} {M.nnz}\n")     # first token -> num_cols (reference reader)
+        for i, j in zip(r, M.col):
+            f.write(f"{i + 1} {j + 1} 0.5\n")
+
+
+@pytest.mark.parametrize("scale", [9, 12])
+def test_outer_driver_matches_oracle(outer_bin, tmp_path, scale):
+    A = W.rmat(scale, 8, 21)
+    mtx = tmp_path / "a.mtx"
+    write_mtx(mtx, A)
+    out = tmp_path / "c.txt"
+    res = subprocess.run([str(outer_bin), str(mtx), str(mtx), str(out)], capture_output=True,
+                         text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    lines = res.stdout.strip().splitlines()
+    # readMTX prints twice, then "P P", then "nnzC nnzCf"
+    ones = W.Csr(A.rows, A.cols, A.rowptr, A.col, np.full(A.nnz, 1.1, np.float32))
+    a = ones.to_csc()
+    ref = oracle.spgemm(A.rows, A.cols, a.colptr, a.rowidx, a.val, ones.rowptr, ones.col, ones.val,
+                        stats=True)
+    p1, p2 = map(int, lines[2].split())
+    assert p1 == p2 == ref["products"]
+    nnzc, nnzcf = map(int, lines[3].split())
+    assert nnzc == len(ref["col"]) and nnzcf == nnzc
+    data = np.loadtxt(out, skiprows=1, ndmin=2)
+    assert np.array_equal(data[:, 1].astype(np.int64), ref["col"])
+    rows = np.repeat(np.arange(A.rows), np.diff(ref["rowptr"]))
+    assert np.array_equal(data[:, 0].astype(np.int64), rows)
+    tol = 2.0 * (ref["nterms"] * 2.0 ** -24 * ref["absum"] + 2.0 ** -24 * np.abs(ref["val"])) + 1e-6
+    assert (np.abs(data[:, 2] - ref["val"]) <= tol).all()
+
+
+def test_unsorted_coo_reported(outer_bin, tmp_path):
+    """cudaCOO2CM on triplets that skip sortCOO: the protocol requires
+    sorted input; the library reports it instead of building a bad CSC."""
+    import ctypes as C
+    L = sg.lib()
+    L.spgemm_set_exit_on_error(0)
+    L.spgemm_set_verbose(0)
+    trip = (sg.Triplet * 3)((2, 0, 1.0), (0, 1, 2.0), (1, 0, 3.0))
+    coo = sg.COO(C.cast(trip, C.POINTER(sg.Triplet)), 3, 3, 3, sg.ROW_MAJOR)
+    L.cudaCOO2CM(coo)
+    assert L.spgemm_legacy_status() == 1
+    L.spgemm_set_exit_on_error(1)
+    L.spgemm_set_verbose(1)
