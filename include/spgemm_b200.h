@@ -144,6 +144,31 @@ int spgemm_reset_kernel_times(spgemm_handle_t handle);
 int spgemm_get_kernel_times(spgemm_handle_t handle, char* names, int names_len,
                             double* ms, long long* launches, int max_kernels);
 
+/* Allocation-free COO -> compressed conversion. This entry point has no
+ * counterpart in the reference; it performs the conversion of cudaCOO2CM
+ * (sorted triplets -> CSR for ROW_MAJOR, CSC for COL_MAJOR) on device arrays
+ * the caller owns, for callers that cannot allocate device memory at that
+ * point: work recorded into a CUDA graph, code whose device memory is owned by
+ * another allocator, latency-critical loops in which a cudaMalloc would
+ * synchronise the device.
+ *   d_triplets: nnz triplets on the device, sorted by (major, minor) index;
+ *   d_ptr: (major dimension + 1) ints; d_idx, d_val: nnz entries each.
+ * Nothing is allocated: the counts are accumulated in d_ptr itself and the
+ * scan's scratch is a fixed static device array of about 131 KB, present on
+ * every GPU that loads this library until the process exits. It limits the
+ * major dimension to SPGEMM_NOALLOC_MAX_MAJOR (larger: SPGEMM_ERR_TOO_LARGE,
+ * nothing launched). The first call on a device looks up that array's device
+ * address (and loads the kernels); make that first call before any stream
+ * capture. All calls share the array: calls that can overlap on the GPU (on
+ * different streams without ordering) race and must not be issued.
+ * Asynchronous on `stream` unless nnz_check is non-null, in which case the
+ * stream is synchronised, *nnz_check receives the number of entries counted,
+ * and an out-of-range index or unsorted input returns SPGEMM_ERR_INVALID. */
+#define SPGEMM_NOALLOC_MAX_MAJOR (1 << 26)
+int spgemm_coo_to_cm_noalloc(const triplet* d_triplets, int nnz, int num_rows,
+                             int num_cols, int type, int* d_ptr, int* d_idx,
+                             float* d_val, void* stream, long long* nnz_check);
+
 /* Companion of the mm.h shims: copy the C that cudaMergeGEMM produced into
  * malloc'd host arrays (sorted CSR, nnz = exact nnz(C)). Returns 0 on
  * success. The reference never returns C (src/mm.cu:420-449). */

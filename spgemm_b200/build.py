@@ -30,6 +30,7 @@ SOURCES = [
     "host_cm.cpp",
     "host_legacy.cpp",
     "legacy_spgemm.cu",
+    "noalloc.cu",
 ]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-Wall", f"-I{INCLUDE}"]
