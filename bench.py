@@ -96,7 +96,8 @@ def build_workload(args):
 
 
 def product_stats(A, B):
-    """Per-row P_i, nnz(A(i,:)) and the B bytes touched (for the roofline)."""
+    """Per-row P_i, nnz(A(i,:)), the column span of the row's products, and the
+    B bytes touched (for the roofline)."""
     deg_b = np.diff(B.rowptr).astype(np.int64)
     rows_of = np.repeat(np.arange(A.rows), np.diff(A.rowptr))
     p_i = np.zeros(A.rows, np.int64)
@@ -104,38 +105,52 @@ def product_stats(A, B):
     touched_k = np.zeros(B.rows, bool)
     touched_k[A.col] = True
     b_touched = 4 * (B.rows + 1) + 8 * int(deg_b[touched_k].sum())
-    return p_i, np.diff(A.rowptr).astype(np.int64), b_touched
+    nonempty = deg_b > 0
+    first = np.full(B.rows, np.iinfo(np.int64).max)
+    last = np.full(B.rows, -1)
+    first[nonempty] = B.col[B.rowptr[:-1][nonempty]]
+    last[nonempty] = B.col[B.rowptr[1:][nonempty] - 1]
+    lo = np.full(A.rows, np.iinfo(np.int64).max)
+    hi = np.full(A.rows, -1)
+    np.minimum.at(lo, rows_of, first[A.col])
+    np.maximum.at(hi, rows_of, last[A.col])
+    span = np.where(p_i > 0, hi + 1 - (lo & ~31), 0)
+    return p_i, np.diff(A.rowptr).astype(np.int64), b_touched, span
 
 
-def sym_bin(p, n):
-    u = np.minimum(p, n)
-    lg = np.maximum(np.ceil(np.log2(np.maximum(2 * u, 1))).astype(np.int64), 6)
-    b = np.where((p <= 1024) & (lg <= 10), lg - 6, np.maximum(lg, 11) - 11 + 5)
-    b = np.where(p > 4096, 8, b)
+# Mirrors of the engine's default bin rules (kernels.cuh), used only to
+# attribute algorithmic bytes to the kernel that processed each row.
+LONG_P, WARP_CAP, WARP_TMAX, MID_COLS, LONG_O, MID_O = 4096, 2048, 256, 1 << 18, 4096, 256
+
+
+def first_bin(p, cap, span):
+    lg = np.ceil(np.log2(np.maximum(cap + cap // 4 + 1, 1))).astype(np.int64)
+    warp = np.clip(lg, 6, int(np.log2(WARP_TMAX))) - 6
+    blk = np.maximum(np.ceil(np.log2(np.maximum(2 * cap, 1))).astype(np.int64), 11) - 11 + 5
+    b = np.where(cap <= WARP_CAP, warp, np.where(span <= MID_COLS, 8, blk))
+    b = np.where(p > LONG_P, 9, b)
     return np.where(p <= 0, -1, b)
 
 
-def num_bin(o, p):
-    lg = np.maximum(np.ceil(np.log2(np.maximum(2 * o, 1))).astype(np.int64), 6)
-    b = np.where((p <= 2048) & (lg <= 9), lg - 6, np.maximum(lg, 10) - 10 + 4)
-    b = np.where(o > 4096, 8, b)
-    return np.where(o <= 0, -1, b)
-
-
-def kernel_bin(name):
-    """(pass, bin) of an engine kernel name, or None."""
+def kernel_rows(name, p_i, o_i, span, n):
+    """Rows processed by an engine kernel (mask), and whether it writes C."""
     import re
-    m = re.match(r"k_(sym|num)_(warp|block)<(\d+)>", name)
+    cap = np.minimum(np.minimum(p_i, n), span)
+    fb = first_bin(p_i, cap, span)
+    long_rows = p_i > LONG_P
+    if name == "k_sym_long":
+        return long_rows, False
+    if name == "k_num_long":
+        return long_rows & (o_i > LONG_O), True
+    if name == "k_num_mid":
+        return long_rows & (o_i > MID_O) & (o_i <= LONG_O) & (span <= MID_COLS), True
+    if name == "k_fused_mid":
+        return fb == 8, True
+    m = re.match(r"k_fused_(warp|block)<(\d+)>", name)
     if m:
-        lg = int(m.group(3))
-        if m.group(1) == "sym":
-            return ("sym", lg - 6 if m.group(2) == "warp" else lg - 11 + 5)
-        return ("num", lg - 6 if m.group(2) == "warp" else lg - 10 + 4)
-    if name.startswith("k_sym_long"):
-        return ("sym", 8)
-    if name.startswith("k_num_long"):
-        return ("num", 8)
-    return None
+        lg = int(m.group(2))
+        return fb == (lg - 6 if m.group(1) == "warp" else lg - 11 + 5), True
+    return None, False
 
 
 def algorithmic_bytes(rows_sel, p_i, a_len, o_i, b_touched, p_total, with_c=True):
@@ -219,7 +234,7 @@ def cpu_baseline(A, B, target_seconds, seed=0):
     import oracle
     a = A.to_csc()
     threads = os.cpu_count() or 1
-    p_i, _, _ = product_stats(A, B)
+    p_i = product_stats(A, B)[0]
     rng = np.random.default_rng(seed)
     order = rng.permutation(A.rows).astype(np.int32)
     csum = np.cumsum(p_i[order])
@@ -325,7 +340,6 @@ def main():
             AP = h1.multiply(A_cm, P_cm)
             h2.multiply(PT_cm, AP)
         ap_nnz = 0
-        p1 = product_stats(A, P)[0].sum()
         flops_per_step = None
     else:
         A, B = wl["products"][0]
@@ -402,28 +416,27 @@ def main():
     roof, pipeline = None, None
     if args.workload != "galerkin" and rank == 0:
         A, B = wl["products"][0]
-        p_i, a_len, b_touched = product_stats(A, B)
+        p_i, a_len, b_touched, span = product_stats(A, B)
         crow = out["rowptr"].cpu().numpy()
         o_i = np.diff(crow.astype(np.int64))
         total_alg = algorithmic_bytes(np.ones(A.rows, bool), p_i, a_len, o_i, b_touched, products)
-        pipeline = {"algorithmic_bytes": total_alg, "gbs": total_alg / (total_ms / args.steps / 1e3) / 1e9 / world,
-                    "frac": total_alg / (total_ms / args.steps / 1e3) / 1e9 / world / peak}
+        step_s = total_ms / args.steps / 1e3
+        pipeline = {"algorithmic_bytes": total_alg, "gbs": total_alg / step_s / 1e9 / world,
+                    "frac": total_alg / step_s / 1e9 / world / peak,
+                    "kernel_ms_per_step": {k: v[0] / args.steps for k, v in
+                                           sorted(ktimes.items(), key=lambda kv: -kv[1][0])}}
         dom = max(ktimes.items(), key=lambda kv: kv[1][0]) if ktimes else None
         if dom:
             name, (ms, cnt) = dom
-            kb = kernel_bin(name)
-            if kb:
-                pas, b = kb
-                sel = (sym_bin(p_i, B.cols) == b) if pas == "sym" else (num_bin(o_i, p_i) == b)
-                alg = algorithmic_bytes(sel, p_i, a_len, o_i, b_touched, products,
-                                        with_c=(pas == "num"))
+            sel, writes_c = kernel_rows(name, p_i, o_i, span, B.cols)
+            if sel is not None:
+                alg = algorithmic_bytes(sel, p_i, a_len, o_i, b_touched, products, with_c=writes_c)
                 per_launch = alg * args.steps / cnt
                 avg_s = ms / cnt / 1e3
                 roof = {"bound": "hbm", "kernel": name, "achieved": per_launch / avg_s / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": per_launch / avg_s / 1e9 / peak,
                         "traffic": None, "algorithmic_bytes_per_launch": per_launch,
                         "avg_launch_ms": ms / cnt, "peak_kind": peak_kind}
-        pipeline["kernel_ms_per_step"] = {k: v[0] / args.steps for k, v in sorted(ktimes.items(), key=lambda kv: -kv[1][0])}
 
     # e2e through the host-buffer C ABI (pinned host memory)
     e2e = None

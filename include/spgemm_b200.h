@@ -56,32 +56,40 @@ typedef struct spgemm_context* spgemm_handle_t;
 typedef struct spgemm_stats {
     long long intermediate_products;   /* P = sum_k nnz(A(:,k)) * nnz(B(k,:)) */
     long long nnz_c;                   /* exact nnz(C) */
-    int rows_per_symbolic_bin[16];     /* rows handled by each symbolic bin */
-    int rows_per_numeric_bin[16];      /* rows handled by each numeric bin */
+    int rows_per_symbolic_bin[16];     /* rows per first-pass bin: 0..4 warp hash
+                                          (64..1024 slots), 5..7 block hash
+                                          (2048..8192), 8 span bitmap, 9 long */
+    int rows_per_numeric_bin[16];      /* long rows per numeric bin: 4..7 block
+                                          hash, 8 column slices, 9 span bitmap */
     int long_row_slices;               /* column slices of the long-row path */
     long long kernel_launches;         /* engine kernels launched by the handle so far */
+    int warp_overflow_rows;            /* warp-bin rows redone by a block kernel */
 } spgemm_stats;
 
 /* Bin thresholds and slice shapes of the engine (spgemm_get_tuning returns
- * the defaults of a new handle). Row i has P_i partial products and nnz_i
- * outputs; a "long" row is handled by column-slice blocks with a presence
- * bitmap instead of a shared-memory hash table. */
+ * the defaults of a new handle). Row i of C has P_i partial products, nnz_i
+ * outputs and a column bound cap_i = min(P_i, columns of C, column span of its
+ * products). Rows with P_i <= long_p are computed in one fused pass: one warp
+ * per row with a hash table of at most warp_table_max slots (a row with more
+ * distinct columns than 4/5 of its table is redone by a block), or one block
+ * per row with a bitmap over the column span (span <= mid_cols) or a larger
+ * hash table. Rows with P_i > long_p take two passes: a bitmap count, then
+ * column-slice blocks (nnz_i > long_o_num), a span bitmap block
+ * (nnz_i > mid_o_min) or a block hash table. */
 typedef struct spgemm_tuning {
-    int warp_p_max_sym;   /* symbolic: one warp per row when P_i <= this */
-    int warp_p_max_num;   /* numeric: one warp per row when P_i <= this */
-    int long_p_sym;       /* symbolic: bitmap (long) path when P_i > this (<= 4096) */
-    int long_o_num;       /* numeric: slice (long) path when nnz_i > this
-                             (>= long_p_sym, <= 4096) */
-    int slice_cap;        /* max outputs per numeric slice; 0 = shared-memory limit */
-    int slice_cols;       /* max columns per numeric slice (multiple of 2048) */
+    int warp_p_max;       /* fused warp path only when P_i <= this */
+    int warp_table_max;   /* largest per-warp hash table: power of two, 64..1024 */
+    int warp_cap_max;     /* rows with cap_i above this skip the warp path */
+    int long_p;           /* two-pass long path when P_i > this (1..4096) */
+    int long_o_num;       /* long rows: column slices when nnz_i > this (1..4096) */
+    int slice_cap;        /* max outputs per column slice; 0 = shared-memory limit */
+    int slice_cols;       /* max columns per column slice (multiple of 2048) */
     int sym_window;       /* columns per symbolic bitmap window (multiple of 2048,
                              <= 2^20) */
     int keep_bitmaps;     /* 1: keep the long rows' symbolic bitmaps (device memory
                              permitting) so the numeric pass skips rebuilding them */
-    int mid_o_min;        /* numeric: rows with mid_o_min < nnz_i <= long_o_num whose
-                             column span is at most mid_cols take the bitmap kernel
-                             instead of a hash table + sort */
-    int mid_cols;         /* (<= 2^18) */
+    int mid_o_min;        /* long rows: span bitmap when nnz_i > this (else hash) */
+    int mid_cols;         /* bitmap paths need a column span <= this (<= 2^18) */
 } spgemm_tuning;
 
 /* Library version string. */

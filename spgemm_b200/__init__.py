@@ -58,10 +58,10 @@ class COO(C.Structure):
 
 class Tuning(C.Structure):
     """spgemm_tuning (include/spgemm_b200.h)."""
-    _fields_ = [("warp_p_max_sym", C.c_int), ("warp_p_max_num", C.c_int),
-                ("long_p_sym", C.c_int), ("long_o_num", C.c_int), ("slice_cap", C.c_int),
-                ("slice_cols", C.c_int), ("sym_window", C.c_int), ("keep_bitmaps", C.c_int),
-                ("mid_o_min", C.c_int), ("mid_cols", C.c_int)]
+    _fields_ = [("warp_p_max", C.c_int), ("warp_table_max", C.c_int),
+                ("warp_cap_max", C.c_int), ("long_p", C.c_int), ("long_o_num", C.c_int),
+                ("slice_cap", C.c_int), ("slice_cols", C.c_int), ("sym_window", C.c_int),
+                ("keep_bitmaps", C.c_int), ("mid_o_min", C.c_int), ("mid_cols", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -70,7 +70,8 @@ class Tuning(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("intermediate_products", C.c_longlong), ("nnz_c", C.c_longlong),
                 ("rows_per_symbolic_bin", C.c_int * 16), ("rows_per_numeric_bin", C.c_int * 16),
-                ("long_row_slices", C.c_int), ("kernel_launches", C.c_longlong)]
+                ("long_row_slices", C.c_int), ("kernel_launches", C.c_longlong),
+                ("warp_overflow_rows", C.c_int)]
 
 
 _lib = None
@@ -199,7 +200,8 @@ class Handle:
         s = Stats()
         self._check(lib().spgemm_get_stats(self._h, C.byref(s)))
         return {"intermediate_products": s.intermediate_products, "nnz_c": s.nnz_c,
-                "rows_per_symbolic_bin": list(s.rows_per_symbolic_bin)[:9],
+                "rows_per_symbolic_bin": list(s.rows_per_symbolic_bin)[:10],
+                "warp_overflow_rows": s.warp_overflow_rows,
                 "rows_per_numeric_bin": list(s.rows_per_numeric_bin)[:10],
                 "long_row_slices": s.long_row_slices, "kernel_launches": s.kernel_launches}
 

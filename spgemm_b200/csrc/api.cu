@@ -95,9 +95,10 @@ int spgemm_set_precision(spgemm_handle_t h, int precision) {
 int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
   if (!h || !out) return SPGEMM_ERR_INVALID;
   const sg::Tuning& t = h->eng.tuning();
-  out->warp_p_max_sym = t.warp_p_max_sym;
-  out->warp_p_max_num = t.warp_p_max_num;
-  out->long_p_sym = t.long_p_sym;
+  out->warp_p_max = t.warp_p_max;
+  out->warp_table_max = t.warp_table_max;
+  out->warp_cap_max = t.warp_cap_max;
+  out->long_p = t.long_p;
   out->long_o_num = t.long_o_num;
   out->slice_cap = t.slice_cap;
   out->slice_cols = t.slice_cols;
@@ -111,9 +112,10 @@ int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
 int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
   if (!h || !in) return SPGEMM_ERR_INVALID;
   sg::Tuning t;
-  t.warp_p_max_sym = in->warp_p_max_sym;
-  t.warp_p_max_num = in->warp_p_max_num;
-  t.long_p_sym = in->long_p_sym;
+  t.warp_p_max = in->warp_p_max;
+  t.warp_table_max = in->warp_table_max;
+  t.warp_cap_max = in->warp_cap_max;
+  t.long_p = in->long_p;
   t.long_o_num = in->long_o_num;
   t.slice_cap = in->slice_cap;
   t.slice_cols = in->slice_cols;
@@ -149,7 +151,8 @@ int spgemm_get_stats(spgemm_handle_t h, spgemm_stats* out) {
   const sg::Engine& E = h->eng;
   out->intermediate_products = E.intermediate_products();
   out->nnz_c = E.nnz_c();
-  for (int b = 0; b < sg::SB_COUNT; ++b) out->rows_per_symbolic_bin[b] = E.sym_bin_rows(b);
+  for (int b = 0; b < sg::FB_COUNT; ++b) out->rows_per_symbolic_bin[b] = E.sym_bin_rows(b);
+  out->warp_overflow_rows = E.overflow_rows();
   for (int b = 0; b < sg::NB_COUNT; ++b) out->rows_per_numeric_bin[b] = E.num_bin_rows(b);
   out->long_row_slices = E.slices();
   out->kernel_launches = E.launches();

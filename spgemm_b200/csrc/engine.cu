@@ -36,16 +36,17 @@ void DevBuf::release() {
 
 Tuning default_tuning() {
   Tuning t;
-  t.warp_p_max_sym = 1024;
-  t.warp_p_max_num = 2048;
-  t.long_p_sym = 4096;
+  t.warp_p_max = 4096;
+  t.warp_table_max = 256;
+  t.warp_cap_max = 2048;
+  t.long_p = 4096;
   t.long_o_num = 4096;
   t.slice_cap = 0;          // 0: as many as the shared-memory budget allows
+  t.slice_cols = 1 << 18;
+  t.sym_window = 1 << 20;
   t.keep_bitmaps = 1;
   t.mid_o_min = 256;
   t.mid_cols = 1 << 18;
-  t.slice_cols = 1 << 18;
-  t.sym_window = 1 << 20;
   return t;
 }
 
@@ -107,6 +108,7 @@ Engine::~Engine() {
   DevBuf* all[] = {&a_rowptr_, &a_col_, &a_val_, &cursor_, &aoff_, &row_p_, &c_cnt_,
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
                    &chunk_cnt_, &slices_buf_, &mid_slices_, &row_span_, &counters_, &restrict_scratch_,
+                   &tcap_, &toff_, &t_col_, &t_val_,
                    &bitmaps_, &out_rowptr_,
                    &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
@@ -130,18 +132,18 @@ int Engine::cuda_fail(cudaError_t e, const char* what) {
 }
 
 int Engine::set_tuning(const Tuning& t) {
-  // numeric long rows read the chunk counts that only symbolic long rows
-  // write, so every numeric long row must have been a symbolic long row
-  if (t.long_o_num < t.long_p_sym) return fail(1, "tuning: long_o_num < long_p_sym");
-  if (t.long_p_sym > 4096 || t.long_o_num > 4096)
-    return fail(1, "tuning: hash bins hold at most 4096 distinct columns");
+  // numeric long rows read the chunk counts and bitmaps that only symbolic
+  // long rows write, and the fused tables hold at most 4096 distinct columns
+  if (t.long_p < 1 || t.long_p > 4096) return fail(1, "tuning: 1 <= long_p <= 4096");
+  if (t.long_o_num < 1 || t.long_o_num > 4096) return fail(1, "tuning: 1 <= long_o_num <= 4096");
+  if (t.warp_table_max < 64 || t.warp_table_max > 1024 || (t.warp_table_max & (t.warp_table_max - 1)))
+    return fail(1, "tuning: warp_table_max must be a power of two in [64, 1024]");
+  if (t.warp_p_max < 0 || t.warp_cap_max < 0) return fail(1, "tuning: warp limits");
   if (t.slice_cols < CHUNK_COLS || t.slice_cols % CHUNK_COLS) return fail(1, "tuning: slice_cols");
   if (t.sym_window < CHUNK_COLS || t.sym_window % CHUNK_COLS || t.sym_window > (1 << 20))
     return fail(1, "tuning: sym_window");
-  if (t.warp_p_max_sym < 0 || t.warp_p_max_num < 0) return fail(1, "tuning: warp limits");
   if (t.slice_cap != 0 && t.slice_cap < CHUNK_COLS)
     return fail(1, "tuning: slice_cap must be 0 (auto) or >= 2048");
-  if (t.long_p_sym < 1) return fail(1, "tuning: long_p_sym");
   if (t.mid_o_min < 0 || t.mid_cols < 0 || t.mid_cols > (1 << 18))
     return fail(1, "tuning: mid_o_min >= 0 and 0 <= mid_cols <= 2^18");
   tn_ = t;
@@ -259,11 +261,9 @@ int Engine::analyze(const cm& A, const cm& B) {
     else
       k_validate<<<vb, 256, 0, stream_>>>(A.ptr, m, A.idx, nnz_a, kdim_, 0, &dc->status);
     SG_LAUNCHED("k_validate(A)");
-    // Later kernels index with these values, so stop here if they are bad.
-    SG_CK(cudaMemcpyAsync(&host_counters_->status, &dc->status, sizeof(unsigned),
-                          cudaMemcpyDeviceToHost, stream_), "read status");
-    SG_CK(cudaStreamSynchronize(stream_), "sync after validation");
-    if (int r = check_status(host_counters_->status)) return r;
+    // The transpose and row analysis guard every index they use; their
+    // verdict and k_validate's are read at the first synchronisation below,
+    // before any kernel trusts the inputs.
   }
 
   // ---- A in CSR ----
@@ -309,26 +309,32 @@ int Engine::analyze(const cm& A, const cm& B) {
   // ---- row analysis ----
   SG_CK(aoff_.ensure(sizeof(int) * (size_t)std::max(nnz_a, 1)), "alloc aoff");
   SG_CK(row_p_.ensure(sizeof(long long) * (size_t)std::max(m, 1)), "alloc row_p");
-  SG_CK(sym_rows_.ensure(sizeof(int) * (size_t)SB_COUNT * std::max(m, 1)), "alloc sym_rows");
+  SG_CK(sym_rows_.ensure(sizeof(int) * (size_t)FB_COUNT * std::max(m, 1)), "alloc bin lists");
   SG_CK(row_span_.ensure(sizeof(int2) * (size_t)std::max(m, 1)), "alloc row spans");
+  SG_CK(tcap_.ensure(sizeof(int) * (size_t)std::max(m, 1)), "alloc row bounds");
+  SG_CK(toff_.ensure(sizeof(long long) * ((size_t)m + 1)), "alloc temp offsets");
   const int vec_ok = ((reinterpret_cast<uintptr_t>(B.idx) | reinterpret_cast<uintptr_t>(B.val)) & 15) == 0;
-  op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_, vec_ok};
+  op_ = Operands{a_rowptr, a_col, a_val, aoff_.as<int>(), B.ptr, B.idx, B.val, m_, kdim_, n_,
+                 vec_ok, B.nnz};
   if (m > 0) {
     prof_begin("k_row_analysis");
     k_row_analysis<<<(m + RA_ROWS - 1) / RA_ROWS, RA_THREADS, 0, stream_>>>(
-        op_, aoff_.as<int>(), row_p_.as<long long>(), c_cnt_.as<int>(), dc->sym_count,
-        sym_rows_.as<int>(), &dc->p_total, &dc->max_row_len, row_span_.as<int2>(), &dc->status,
-        tn_);
+        op_, aoff_.as<int>(), row_p_.as<long long>(), c_cnt_.as<int>(), tcap_.as<int>(),
+        dc->fb_count, sym_rows_.as<int>(), &dc->p_total, &dc->max_row_len, row_span_.as<int2>(),
+        &dc->status, tn_);
     SG_LAUNCHED("k_row_analysis");
   }
+  // temporary-buffer slots of the fused rows (grand total = buffer size)
+  if (int r = scan_counts(tcap_.as<int>(), m, toff_.as<long long>())) return r;
   SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
         "read counters");
   SG_CK(cudaStreamSynchronize(stream_), "sync after row analysis");
   if (int r = check_status(host_counters_->status)) return r;
   p_total_ = (long long)host_counters_->p_total;
-  for (int b = 0; b < SB_COUNT; ++b) sym_counts_[b] = host_counters_->sym_count[b];
-  n_long_sym_ = sym_counts_[SB_LONG];
+  for (int b = 0; b < FB_COUNT; ++b) fb_counts_[b] = host_counters_->fb_count[b];
+  n_long_sym_ = fb_counts_[FB_LONG];
   max_row_len_ = host_counters_->max_row_len;
+  temp_total_ = host_counters_->grand_total;
   n_chunks_ = (n_ + CHUNK_COLS - 1) / CHUNK_COLS;
   have_analysis_ = true;
   return 0;
@@ -340,20 +346,22 @@ int Engine::symbolic_pass(long long* nnz_c) {
   const int m = m_;
   DevCounters* dc = counters_.as<DevCounters>();
 
-  // ---- symbolic pass ----
+  // ---- first pass: fused rows to the temporary buffer, long rows counted ----
+  SG_CK(t_col_.ensure(sizeof(int) * (size_t)std::max(temp_total_, 1ll)), "alloc temp columns");
+  SG_CK(t_val_.ensure(sizeof(float) * (size_t)std::max(temp_total_, 1ll)), "alloc temp values");
   if (n_long_sym_ > 0) {
     SG_CK(long_slot_.ensure(sizeof(int) * (size_t)std::max(m, 1)), "alloc long_slot");
     SG_CK(chunk_cnt_.ensure(sizeof(int) * (size_t)n_long_sym_ * std::max(n_chunks_, 1)),
           "alloc chunk counts");
   }
-  if (int r = launch_symbolic_bins()) return r;
+  if (int r = launch_first_pass()) return r;
 
-  // ---- row pointers + numeric binning ----
+  // ---- row pointers + numeric binning of the long rows ----
   if (int r = scan_counts(c_cnt_.as<int>(), m, c_rowptr64_.as<long long>())) return r;
   SG_CK(num_rows_.ensure(sizeof(int) * (size_t)NB_COUNT * std::max(m, 1)), "alloc num_rows");
   big_capacity_ = (long long)n_long_sym_ * std::max(n_chunks_, 1);
   SG_CK(slices_buf_.ensure(sizeof(Slice) * (size_t)std::max(big_capacity_, 1ll)), "alloc slices");
-  SG_CK(mid_slices_.ensure(sizeof(Slice) * (size_t)std::max(m, 1)), "alloc mid slices");
+  SG_CK(mid_slices_.ensure(sizeof(Slice) * (size_t)std::max(n_long_sym_, 1)), "alloc mid slices");
   // output capacity of one big slice: what the shared-memory budget leaves
   Tuning tr = tn_;
   {
@@ -365,7 +373,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
     tr.slice_cap = (int)cap;
     tn_run_slice_cap_ = tr.slice_cap;
   }
-  if (m > 0) {
+  if (m > 0 && n_long_sym_ > 0) {
     prof_begin("k_num_bin");
     k_num_bin<<<(m + NBIN_THREADS - 1) / NBIN_THREADS, NBIN_THREADS, 0, stream_>>>(
         m, n_, c_cnt_.as<int>(), row_p_.as<long long>(), c_rowptr64_.as<long long>(),
@@ -383,6 +391,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
   for (int b = 0; b < NB_COUNT; ++b) num_counts_[b] = host_counters_->num_count[b];
   nslices_ = host_counters_->slice_count;
   nmid_ = host_counters_->mid_count;
+  overflow_rows_ = host_counters_->overflow_count;
   if (nnz_c_ > 2147483647ll)
     return fail(4, "nnz(C) = " + std::to_string(nnz_c_) + " exceeds the int32 range of cm");
   if (nnz_c) *nnz_c = nnz_c_;
@@ -390,21 +399,21 @@ int Engine::symbolic_pass(long long* nnz_c) {
   return 0;
 }
 
-int Engine::launch_symbolic_bins() {
+int Engine::launch_first_pass() {
   const Operands op = op_;
-  unsigned* status = &counters_.as<DevCounters>()->status;
+  DevCounters* dc = counters_.as<DevCounters>();
+  unsigned* status = &dc->status;
   const int m = m_;
   int* c_cnt = c_cnt_.as<int>();
   const long long* row_p = row_p_.as<long long>();
-  const int* rows = sym_rows_.as<int>();
-  constexpr int WPB = SW_THREADS / 32;
+  int* rows = sym_rows_.as<int>();
   bitmap_words_ = 0;
   // long rows first: they are the heaviest work items
-  if (sym_counts_[SB_LONG] > 0) {
+  if (fb_counts_[FB_LONG] > 0) {
     const int win = std::min(n_, tn_.sym_window);
     const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)((win + 31) / 32) * 4;
     SG_CK(smem_attr(k_sym_long, smem), "smem attr k_sym_long");
-    const int cnt = sym_counts_[SB_LONG];
+    const int cnt = fb_counts_[FB_LONG];
     const int grid = blocks_for(cnt, 1, (long long)sms_ * 2);
     const int stride = 2 * max_row_len_ + 2;
     if (n_ > tn_.sym_window)
@@ -424,45 +433,100 @@ int Engine::launch_symbolic_bins() {
     }
     prof_begin("k_sym_long");
     k_sym_long<<<grid, LONG_THREADS, smem, stream_>>>(
-        op, rows + (size_t)SB_LONG * m, cnt, row_p, c_cnt, long_slot_.as<int>(),
+        op, rows + (size_t)FB_LONG * m, cnt, row_p, c_cnt, long_slot_.as<int>(),
         chunk_cnt_.as<int>(), n_chunks_, restrict_scratch_.as<int>(), stride,
         bitmaps_.as<unsigned>(), bitmap_words_, status, tn_);
     SG_LAUNCHED("k_sym_long");
   }
-#define SG_SYM_WARP(L)                                                                    \
-  {                                                                                        \
-    const int b = L - 6, cnt = sym_counts_[b];                                             \
-    if (cnt > 0) {                                                                         \
-      const size_t smem = WPB * ((size_t(1) << L) * 4 + SEG_SCRATCH_BYTES);                \
-      SG_CK(smem_attr(k_sym_warp<L>, smem), "smem attr k_sym_warp");                       \
-      prof_begin("k_sym_warp<" #L ">");                                                            \
-      k_sym_warp<L><<<blocks_for(cnt, WPB, (long long)sms_ * 8), SW_THREADS, smem, stream_>>>( \
-          op, rows + (size_t)b * m, cnt, c_cnt, status);                                   \
-      SG_LAUNCHED("k_sym_warp");                                                           \
-    }                                                                                      \
+  return precision_ == 0 ? launch_fused<0>() : launch_fused<1>();
+}
+
+template <int MODE>
+int Engine::launch_fused() {
+  constexpr int WPB = SW_THREADS / 32;
+  constexpr int MID_THREADS = 512;
+  constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
+  const Operands op = op_;
+  DevCounters* dc = counters_.as<DevCounters>();
+  unsigned* status = &dc->status;
+  const int m = m_;
+  int* rows = sym_rows_.as<int>();
+  int* c_cnt = c_cnt_.as<int>();
+  const long long* row_p = row_p_.as<long long>();
+  const long long* toff = toff_.as<long long>();
+  int* t_col = t_col_.as<int>();
+  float* t_val = t_val_.as<float>();
+  int* mid_rows = rows + (size_t)FB_MID * m;
+  int* big_rows = rows + (size_t)(FB_BLOCK0 + 2) * m;
+  int overflow_bound = 0;  // rows the warp bins may push to the mid / block lists
+#define SG_FUSED_WARP(L)                                                                      \
+  {                                                                                            \
+    const int b = L - 6, cnt = fb_counts_[b];                                                  \
+    if (cnt > 0) {                                                                             \
+      overflow_bound += cnt;                                                                   \
+      const size_t smem = WPB * ((size_t(1) << L) * (VB + 4) + SEG_SCRATCH_BYTES);             \
+      SG_CK(smem_attr(k_fused_warp<L, MODE>, smem), "smem attr k_fused_warp");                 \
+      prof_begin("k_fused_warp<" #L ">");                                                      \
+      k_fused_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms_ * 16), SW_THREADS, smem,    \
+                              stream_>>>(op, rows + (size_t)b * m, cnt, row_span_.as<int2>(),  \
+                                         toff, c_cnt, t_col, t_val, mid_rows,                  \
+                                         &dc->fb_count[FB_MID], big_rows,                      \
+                                         &dc->fb_count[FB_BLOCK0 + 2], tn_.mid_cols,           \
+                                         &dc->overflow_count);                                 \
+      SG_LAUNCHED("k_fused_warp");                                                             \
+    }                                                                                          \
   }
-  SG_SYM_WARP(6) SG_SYM_WARP(7) SG_SYM_WARP(8) SG_SYM_WARP(9) SG_SYM_WARP(10)
-#undef SG_SYM_WARP
-#define SG_SYM_BLOCK(L, NT)                                                               \
-  {                                                                                        \
-    const int b = L - 11 + 5, cnt = sym_counts_[b];                                        \
-    if (cnt > 0) {                                                                         \
-      const size_t smem = (size_t(1) << L) * 4 + (NT / 32) * SEG_SCRATCH_BYTES;            \
-      SG_CK(smem_attr(k_sym_block<L, NT>, smem), "smem attr k_sym_block");                 \
-      prof_begin("k_sym_block<" #L ">");                                                       \
-      k_sym_block<L, NT><<<blocks_for(cnt, 1, (long long)sms_ * 8), NT, smem, stream_>>>(  \
-          op, rows + (size_t)b * m, cnt, row_p, c_cnt, status);                            \
-      SG_LAUNCHED("k_sym_block");                                                          \
-    }                                                                                      \
+  SG_FUSED_WARP(6) SG_FUSED_WARP(7) SG_FUSED_WARP(8) SG_FUSED_WARP(9) SG_FUSED_WARP(10)
+#undef SG_FUSED_WARP
+  // mid bitmap rows (and warp overflow with a narrow span)
+  if (fb_counts_[FB_MID] + overflow_bound > 0) {
+    const int width = std::min(n_, tn_.mid_cols) + 32;  // + alignment of lo down to 32
+    const int dir_words = (width + 31) / 32;
+    const int cap = (int)std::min<long long>(tn_.long_p, n_);
+    const size_t smem = (MID_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)dir_words * sizeof(uint2) +
+                        (size_t)cap * 8 + sizeof(unsigned) * ((dir_words + 31) / 32) +
+                        sizeof(int) * (size_t)cap;
+    SG_CK(smem_attr(k_num_long<MODE, MID_THREADS, true>, smem), "smem attr k_num_long fused");
+    const int grid = blocks_for(fb_counts_[FB_MID] + overflow_bound, 1, (long long)sms_ * 4);
+    prof_begin("k_fused_mid");
+    k_num_long<MODE, MID_THREADS, true><<<grid, MID_THREADS, smem, stream_>>>(
+        op, nullptr, 0, row_p, dir_words, cap, restrict_scratch_.as<int>(), 0,
+        bitmaps_.as<unsigned>(), 0, long_slot_.as<int>(), t_col, t_val, status, mid_rows,
+        &dc->fb_count[FB_MID], row_span_.as<int2>(), toff, c_cnt);
+    SG_LAUNCHED("k_fused_mid");
   }
-  SG_SYM_BLOCK(11, 256) SG_SYM_BLOCK(12, 256) SG_SYM_BLOCK(13, 256)
-#undef SG_SYM_BLOCK
+#define SG_FUSED_BLOCK(L, NT)                                                                 \
+  {                                                                                            \
+    const int b = L - 11 + FB_BLOCK0;                                                          \
+    const int bound = fb_counts_[b] + (L == 13 ? overflow_bound : 0);                          \
+    if (bound > 0) {                                                                           \
+      const size_t smem = (size_t(1) << L) * (VB + 4) + (NT / 32) * SEG_SCRATCH_BYTES;         \
+      SG_CK(smem_attr(k_fused_block<L, NT, MODE>, smem), "smem attr k_fused_block");           \
+      prof_begin("k_fused_block<" #L ">");                                                     \
+      k_fused_block<L, NT, MODE><<<blocks_for(bound, 1, (long long)sms_ * 8), NT, smem,         \
+                                   stream_>>>(op, rows + (size_t)b * m, &dc->fb_count[b],      \
+                                              row_p, toff, c_cnt, t_col, t_val, status);       \
+      SG_LAUNCHED("k_fused_block");                                                            \
+    }                                                                                          \
+  }
+  SG_FUSED_BLOCK(11, 256) SG_FUSED_BLOCK(12, 256) SG_FUSED_BLOCK(13, 512)
+#undef SG_FUSED_BLOCK
   return 0;
 }
+
+template int Engine::launch_fused<0>();
+template int Engine::launch_fused<1>();
 
 int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
   if (!c_rowptr || (nnz_c_ > 0 && (!c_col || !c_val))) return fail(1, "null output pointer");
+  if (m_ > 0 && temp_total_ > 0) {
+    prof_begin("k_copy_fused");
+    k_copy_fused<<<blocks_for((long long)m_ * 32, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+        m_, tcap_.as<int>(), toff_.as<long long>(), c_cnt_.as<int>(), c_rowptr64_.as<long long>(),
+        t_col_.as<int>(), t_val_.as<float>(), c_col, c_val);
+    SG_LAUNCHED("k_copy_fused");
+  }
   if (int r = launch_numeric_bins(c_col, c_val)) return r;
   prof_begin("k_rowptr_to_i32");
   k_rowptr_to_i32<<<blocks_for(m_ + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
@@ -510,10 +574,10 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     k_num_long<MODE, LONG_THREADS, false><<<grid, LONG_THREADS, smem, stream_>>>(
         op, slices_buf_.as<Slice>(), nslices_, row_p, dir_words, tn_run_slice_cap_,
         restrict_scratch_.as<int>(), stride, bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), c_col, c_val, status);
+        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr);
     SG_LAUNCHED("k_num_long");
   }
-  // mid bitmap slices: whole rows of at most long_o_num outputs, 512 threads
+  // mid bitmap slices of long rows: at most long_o_num outputs, 512 threads
   if (nmid_ > 0) {
     const int width = std::min(n_, tn_.mid_cols) + 32;  // + alignment of lo down to 32
     const int dir_words = (width + 31) / 32;            // <= 8193, so l1 fits 512 threads
@@ -527,24 +591,9 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     k_num_long<MODE, MID_THREADS, true><<<grid, MID_THREADS, smem, stream_>>>(
         op, mid_slices_.as<Slice>(), nmid_, row_p, dir_words, cap,
         restrict_scratch_.as<int>(), 0, bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), c_col, c_val, status);
+        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr);
     SG_LAUNCHED("k_num_mid");
   }
-#define SG_NUM_WARP(L)                                                                       \
-  {                                                                                           \
-    const int b = L - 6, cnt = num_counts_[b];                                                \
-    if (cnt > 0) {                                                                            \
-      const size_t smem = WPB * ((size_t(1) << L) * (VB + 4) + SEG_SCRATCH_BYTES);            \
-      SG_CK(smem_attr(k_num_warp<L, MODE>, smem), "smem attr k_num_warp");                    \
-      prof_begin("k_num_warp<" #L ">");                                                        \
-      k_num_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms_ * 8), SW_THREADS, smem,      \
-                            stream_>>>(op, rows + (size_t)b * m, cnt, c_rowptr, c_col, c_val, \
-                                       status);                                               \
-      SG_LAUNCHED("k_num_warp");                                                              \
-    }                                                                                         \
-  }
-  SG_NUM_WARP(6) SG_NUM_WARP(7) SG_NUM_WARP(8) SG_NUM_WARP(9)
-#undef SG_NUM_WARP
 #define SG_NUM_BLOCK(L, NT)                                                                  \
   {                                                                                           \
     const int b = L - 10 + 4, cnt = num_counts_[b];                                           \

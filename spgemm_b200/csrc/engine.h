@@ -26,7 +26,7 @@ struct DevBuf {
 // Device-side counters, reset once per product and read back at the two
 // synchronisation points.
 struct DevCounters {
-  int sym_count[16];
+  int fb_count[16];  // first-pass bins (rows per bin; mid / block lists grow on warp overflow)
   int num_count[16];
   int slice_count;
   int mid_count;
@@ -34,6 +34,7 @@ struct DevCounters {
   unsigned long long p_total;
   long long grand_total;
   int max_row_len;  // longest row of A (entries)
+  int overflow_count;  // warp-bin rows redone by the mid / block kernels
 };
 
 class Engine {
@@ -69,7 +70,8 @@ class Engine {
   long long nnz_c() const { return nnz_c_; }
   int m() const { return m_; }
   int n() const { return n_; }
-  int sym_bin_rows(int b) const { return sym_counts_[b]; }
+  int sym_bin_rows(int b) const { return fb_counts_[b]; }
+  int overflow_rows() const { return overflow_rows_; }
   int num_bin_rows(int b) const { return num_counts_[b]; }
   int slices() const { return nslices_; }
   cudaStream_t stream() const { return stream_; }
@@ -95,7 +97,8 @@ class Engine {
   int cuda_fail(cudaError_t e, const char* what);
 
  private:
-  int launch_symbolic_bins();
+  int launch_first_pass();
+  template <int MODE> int launch_fused();
   int launch_numeric_bins(int* c_col, float* c_val);
   template <int MODE> int launch_numeric_mode(int* c_col, float* c_val);
   size_t big_dir_bytes() const;
@@ -116,7 +119,9 @@ class Engine {
   bool have_sym_ = false;
   int m_ = 0, kdim_ = 0, n_ = 0, n_chunks_ = 0;
   long long p_total_ = 0, nnz_c_ = 0;
-  int sym_counts_[16] = {0};
+  int fb_counts_[16] = {0};
+  long long temp_total_ = 0;
+  int overflow_rows_ = 0;
   int num_counts_[16] = {0};
   int nslices_ = 0, nmid_ = 0;
   long long big_capacity_ = 0;
@@ -128,6 +133,7 @@ class Engine {
   DevBuf a_rowptr_, a_col_, a_val_, cursor_, aoff_;
   DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
   DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_, mid_slices_, row_span_;
+  DevBuf tcap_, toff_, t_col_, t_val_;  // fused pass: row bounds, temp offsets, temp output
   DevBuf counters_, restrict_scratch_, bitmaps_;
   int bitmap_words_ = 0;  // per long row; 0 when the bitmaps are not kept
   int max_row_len_ = 0;

@@ -39,33 +39,44 @@ struct Operands {
   const float* __restrict__ b_val;
   int m, kdim, n;
   int vec_ok;  // b_col and b_val are 16-byte aligned: 128-bit loads allowed
+  int nnz_b;
 };
 
-// Symbolic bins: 0..4 warp-per-row hash (2^6..2^10 slots), 5..7 block-per-row
-// hash (2^11..2^13 slots), 8 long rows (bitmap).
-constexpr int SB_COUNT = 9;
-constexpr int SB_LONG = 8;
-// Numeric bins: 0..3 warp-per-row (2^6..2^9 slots), 4..7 block-per-row
-// (2^10..2^13 slots), 8 long rows (column slices).
+// First-pass bins (k_row_analysis). Rows of at most long_p products are
+// computed in one fused pass (sorted output into a temporary buffer):
+//   0..4  one warp per row, hash table of 2^6..2^10 slots (optimistic: a row
+//         with more distinct columns than 4/5 of the table is redone below)
+//   5..7  one block per row, hash table of 2^11..2^13 slots
+//   8     one block per row, bitmap over the row's column span ("mid")
+// Rows with more products take the two-phase long path:
+//   9     symbolic bitmap count (k_sym_long), numeric later
+constexpr int FB_WARP_BINS = 5;
+constexpr int FB_BLOCK0 = 5;
+constexpr int FB_MID = 8;
+constexpr int FB_LONG = 9;
+constexpr int FB_COUNT = 10;
+// Numeric bins of long rows: 4..7 block hash (2^10..2^13 slots), 8 column
+// slices, 9 bitmap of the whole span (statistics slots 0..3 stay unused).
 constexpr int NB_COUNT = 10;
 constexpr int NB_LONG = 8;
-constexpr int NB_MID = 9;  // mid rows in bitmap slices (counted here for statistics)
+constexpr int NB_MID = 9;
 
 constexpr int CHUNK_COLS = 2048;               // column granularity of slicing
 constexpr int CHUNK_WORDS = CHUNK_COLS / 32;
 constexpr long long FP64_ROW_PARTIALS = 4096;  // compensated mode: FP64 above this
 
 struct Tuning {
-  int warp_p_max_sym;   // symbolic: warp-per-row only when P_i <= this
-  int warp_p_max_num;   // numeric: warp-per-row only when P_i <= this
-  int long_p_sym;       // symbolic: bitmap path when P_i > this
-  int long_o_num;       // numeric: slice path when nnz_i > this (>= long_p_sym)
+  int warp_p_max;       // fused warp path only when P_i <= this
+  int warp_table_max;   // largest per-warp table (64..1024 slots)
+  int warp_cap_max;     // rows whose column bound exceeds this skip the warp path
+  int long_p;           // two-phase long path when P_i > this (<= 4096)
+  int long_o_num;       // long rows: column-slice numeric when nnz_i > this (<= 4096)
   int slice_cap;        // max outputs of one numeric long slice (0: smem budget)
   int slice_cols;       // max columns of one numeric long slice (multiple of 2048)
   int sym_window;       // columns per symbolic bitmap window (multiple of 2048)
   int keep_bitmaps;     // keep long rows' symbolic bitmaps for the numeric pass
-  int mid_o_min;        // numeric: bitmap slice for rows with nnz_i > this ...
-  int mid_cols;         // ... whose column span is at most this many columns
+  int mid_o_min;        // long rows: bitmap numeric when nnz_i > this ...
+  int mid_cols;         // bitmap paths need a column span of at most this (<= 2^18)
 };
 
 __host__ __device__ inline int ceil_log2_ll(long long v) {
@@ -74,23 +85,34 @@ __host__ __device__ inline int ceil_log2_ll(long long v) {
   return r;
 }
 
-__host__ __device__ inline int sym_bin_of(long long p, int n, const Tuning& t) {
-  if (p <= 0) return -1;
-  if (p > t.long_p_sym) return SB_LONG;
-  long long u = p < n ? p : n;
-  int lg = ceil_log2_ll(2 * u);
-  if (lg < 6) lg = 6;
-  if (p <= t.warp_p_max_sym && lg <= 10) return lg - 6;
-  if (lg < 11) lg = 11;
-  return lg - 11 + 5;  // lg <= 13 because u <= long_p_sym <= 4096
+// Column bound of row i: nnz_i <= min(P_i, n, span_i).
+__host__ __device__ inline long long row_cap(long long p, int n, int span) {
+  long long c = p < n ? p : n;
+  return c < span ? c : span;
 }
 
+__host__ __device__ inline int first_bin_of(long long p, long long cap, int span, const Tuning& t) {
+  if (p <= 0) return -1;
+  if (p > t.long_p) return FB_LONG;
+  if (cap <= t.warp_cap_max && p <= t.warp_p_max) {
+    int lg = ceil_log2_ll(cap + cap / 4 + 1);  // table >= 1.25 x column bound
+    if (lg < 6) lg = 6;
+    const int lmax = ceil_log2_ll(t.warp_table_max);
+    if (lg > lmax) lg = lmax;
+    return lg - 6;
+  }
+  if (span <= t.mid_cols) return FB_MID;
+  int lg = ceil_log2_ll(2 * cap);
+  if (lg < 11) lg = 11;
+  return lg - 11 + FB_BLOCK0;  // cap <= p <= long_p <= 4096, so lg <= 13
+}
+
+// Numeric bin of a long row (P_i > long_p) with nnz_i outputs.
 __host__ __device__ inline int num_bin_of(int o, long long p, const Tuning& t) {
+  (void)p;
   if (o <= 0) return -1;
   if (o > t.long_o_num) return NB_LONG;
   int lg = ceil_log2_ll(2ll * o);
-  if (lg < 6) lg = 6;
-  if (p <= t.warp_p_max_num && lg <= 9) return lg - 6;
   if (lg < 10) lg = 10;
   return lg - 10 + 4;  // lg <= 13 because o <= long_o_num <= 4096
 }
@@ -98,6 +120,8 @@ __host__ __device__ inline int num_bin_of(int o, long long p, const Tuning& t) {
 // One column slice of a row for the numeric bitmap kernel.
 constexpr int SLICE_WHOLE = 1;      // the slice holds all of the row's outputs
 constexpr int SLICE_BITS_KEPT = 2;  // the symbolic pass kept the row's bitmap
+constexpr int SLICE_FUSED = 4;      // fused pass: output to the temporary buffer,
+                                    // nnz found here and written to c_cnt
 struct Slice {
   long long out;  // first output position in C
   int row;
@@ -115,6 +139,7 @@ struct SegScratch {
   int bstart[32];
   int len[32];
   float a[32];
+  int count;  // fused warp rows: distinct columns inserted so far
 };
 
 // Move the lanes with len > 0 to lanes 0..cnt-1 (order preserved).
@@ -280,12 +305,17 @@ __device__ __forceinline__ int chunk_for(long long p, int nwarps, int max_chunk)
   return (int)u;
 }
 
-// Whole row of A, one warp.
+// Whole row of A, one warp. With stop_limit >= 0 the walk ends early once
+// sc->count exceeds it (checked between 32-entry batches, warp-uniformly).
 template <bool NEED_VAL, class F>
 __device__ __forceinline__ void warp_expand_row(const Operands& op, int rs, int re,
-                                                F& f, SegScratch* sc) {
+                                                F& f, SegScratch* sc, int stop_limit = -1) {
   const int lane = lane_id();
   for (int base = rs; base < re; base += 32) {
+    if (stop_limit >= 0) {
+      __syncwarp();
+      if (*((volatile int*)&sc->count) > stop_limit) break;
+    }
     const int j = base + lane;
     int bstart = 0, len = 0;
     float a = 0.f;
@@ -574,6 +604,80 @@ struct LongBits {
   }
 };
 
+// Fused-pass hash insert: like the numeric inserts, but a full table is not an
+// error (the caller redoes the row with a larger structure when it counted
+// more distinct columns than its limit), and new keys are counted.
+__device__ __forceinline__ int hash_slot_soft(unsigned* keys, int log2t, unsigned col,
+                                              bool& inserted) {
+  const unsigned mask = (1u << log2t) - 1u;
+  unsigned h = hash_col(col, log2t);
+  inserted = false;
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const unsigned k = ((volatile unsigned*)keys)[h];
+    if (k == col) return (int)h;
+    if (k == EMPTY_KEY) {
+      const unsigned old = atomicCAS(keys + h, EMPTY_KEY, col);
+      if (old == EMPTY_KEY) { inserted = true; return (int)h; }
+      if (old == col) return (int)h;
+    }
+    h = (h + 1u) & mask;
+  }
+  return -1;
+}
+
+// `count` (per warp, shared) counts distinct columns; once it exceeds `limit`
+// the row will be redone elsewhere, so further products are skipped.
+template <int MODE>  // 0: FP32 add; 1: TwoSum-compensated FP32 pair
+struct FusedHash {
+  unsigned* keys;
+  void* vals;
+  int log2t;
+  int* count;
+  int limit;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if (*((volatile int*)count) > limit) return;
+    bool ins;
+    const int h = hash_slot_soft(keys, log2t, (unsigned)col, ins);
+    if (ins) atomicAdd(count, 1);
+    if (h < 0) return;
+    if (MODE == 0) atomicAdd(static_cast<float*>(vals) + h, __fmul_rn(a, b));
+    else twosum_accumulate(static_cast<float2*>(vals) + h, a, b);
+  }
+};
+
+// Bitonic sort of keys/values[0, n) (n a power of two, >= 1) by any number of
+// cooperating threads; Sync synchronises them.
+template <class V, class Sync>
+__device__ __forceinline__ void bitonic_sort_kv_rt(unsigned* keys, V* vals, int n, int tid,
+                                                   int nthreads, Sync sync) {
+  for (int k = 2; k <= n; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (n >> 1); t += nthreads) {
+        const int lo = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        const int hi = lo + j;
+        const bool up = (lo & k) == 0;
+        const unsigned kl = keys[lo], kh = keys[hi];
+        if ((kl > kh) == up) {
+          keys[lo] = kh;
+          keys[hi] = kl;
+          const V vl = vals[lo];
+          vals[lo] = vals[hi];
+          vals[hi] = vl;
+        }
+      }
+      sync();
+    }
+  }
+}
+
+struct LongValTwoSum {
+  const uint2* dir;
+  float2* vals;
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b);
+};
+
 // LongBits that also records, in a second-level bitmap l1 (one bit per
 // directory word), which directory words became non-empty.
 struct LongBitsTracked {
@@ -611,6 +715,10 @@ struct LongValPlain {
     if ((unsigned)(col - lo) < width) atomicAdd(vals + long_slot(dir, lo, col), __fmul_rn(a, b));
   }
 };
+
+__device__ __forceinline__ void LongValTwoSum::operator()(int col, float a, float b) {
+  if ((unsigned)(col - lo) < width) twosum_accumulate(vals + long_slot(dir, lo, col), a, b);
+}
 
 struct LongValF64 {
   const uint2* dir;

@@ -87,20 +87,24 @@ constexpr int RA_ROWS = 64;  // rows per block
 
 // Per row i: P_i = sum over A(i,k) of nnz(B(k,:)) (the intermediate product
 // count the reference accumulates per row in initGEMM, src/mm.cu:138-148),
-// the flattened offset of each A entry, and the symbolic bin. Rows are
-// appended to their bin's list with one global atomic per bin per block.
+// the flattened offset of each A entry, the column span of the row's
+// products, the first-pass bin, and tcap[i] = the column bound min(P_i, n,
+// span_i) for rows the fused pass computes (0 otherwise), which sizes their
+// slot in the temporary output buffer. Rows are appended to their bin's list
+// with one global atomic per bin per block. B's pointers are range-checked
+// here because k_validate's verdict is only read after this kernel.
 __global__ void __launch_bounds__(RA_THREADS)
 k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_p,
-               int* __restrict__ c_cnt, int* __restrict__ sym_count,
-               int* __restrict__ sym_rows, unsigned long long* __restrict__ p_total,
+               int* __restrict__ c_cnt, int* __restrict__ tcap, int* __restrict__ fb_count,
+               int* __restrict__ fb_rows, unsigned long long* __restrict__ p_total,
                int* __restrict__ max_row_len, int2* __restrict__ row_span, unsigned* status,
                Tuning tn) {
-  __shared__ int hist[SB_COUNT], base[SB_COUNT];
+  __shared__ int hist[FB_COUNT], base[FB_COUNT];
   __shared__ int rowbin[RA_ROWS], rowrank[RA_ROWS];
   __shared__ unsigned long long block_p;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * RA_ROWS;
-  if (threadIdx.x < SB_COUNT) hist[threadIdx.x] = 0;
+  if (threadIdx.x < FB_COUNT) hist[threadIdx.x] = 0;
   if (threadIdx.x == 0) block_p = 0;
   __syncthreads();
   for (int lr = warp; lr < RA_ROWS; lr += RA_THREADS / 32) {
@@ -119,10 +123,14 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
         const int k = op.a_col[j];
         if ((unsigned)k < (unsigned)op.kdim) {
           const int bs = op.b_rowptr[k], be = op.b_rowptr[k + 1];
-          len = be - bs;
-          if (be > bs) {
-            lo = min(lo, op.b_col[bs]);
-            hi = max(hi, op.b_col[be - 1]);
+          if (bs >= 0 && be <= op.nnz_b && bs <= be) {
+            len = be - bs;
+            if (be > bs) {
+              lo = min(lo, op.b_col[bs]);
+              hi = max(hi, op.b_col[be - 1]);
+            }
+          } else {
+            atomicOr(status, ST_BAD_INDEX);
           }
         } else {
           atomicOr(status, ST_BAD_INDEX);
@@ -138,25 +146,28 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
       hi = max(hi, __shfl_xor_sync(FULL, hi, d));
     }
     if (lane == 0) {
-      row_span[i] = acc > 0 ? make_int2(lo, hi) : make_int2(0, -1);
       if (re - rs > 0) atomicMax(max_row_len, re - rs);
+      const int span = acc > 0 ? hi + 1 - lo : 0;
+      row_span[i] = acc > 0 ? make_int2(lo, hi) : make_int2(0, -1);
       row_p[i] = acc;
       if (acc >= (1ll << 31)) atomicOr(status, ST_ROW_TOO_LONG);
-      const int bin = sym_bin_of(acc, op.n, tn);
+      const long long cap = row_cap(acc, op.n, span);
+      const int bin = first_bin_of(acc, cap, span, tn);
       if (bin < 0) c_cnt[i] = 0;
+      tcap[i] = (bin >= 0 && bin != FB_LONG) ? (int)cap : 0;
       rowbin[lr] = bin;
       if (bin >= 0) rowrank[lr] = atomicAdd(&hist[bin], 1);
       atomicAdd(&block_p, (unsigned long long)acc);
     }
   }
   __syncthreads();
-  if (threadIdx.x < SB_COUNT && hist[threadIdx.x])
-    base[threadIdx.x] = atomicAdd(sym_count + threadIdx.x, hist[threadIdx.x]);
+  if (threadIdx.x < FB_COUNT && hist[threadIdx.x])
+    base[threadIdx.x] = atomicAdd(fb_count + threadIdx.x, hist[threadIdx.x]);
   if (threadIdx.x == 0) atomicAdd(p_total, block_p);
   __syncthreads();
   for (int lr = threadIdx.x; lr < RA_ROWS; lr += RA_THREADS) {
     const int b = rowbin[lr];
-    if (b >= 0) sym_rows[(size_t)b * op.m + base[b] + rowrank[lr]] = row0 + lr;
+    if (b >= 0) fb_rows[(size_t)b * op.m + base[b] + rowrank[lr]] = row0 + lr;
   }
 }
 
@@ -164,58 +175,154 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
 // Symbolic pass
 // ---------------------------------------------------------------------------
 
+__device__ __forceinline__ long long block_excl_scan64(long long v, long long* shm,
+                                                       long long& total);
+
 constexpr int SW_THREADS = 256;  // warp-per-row kernels: 8 warps per block
 
-template <int LOG2T>
+// Value slot type of each precision mode (0 plain, 1 compensated).
+template <int MODE> struct SlotOf { using T = float; };
+template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or double bits
+
+// Fused pass, one warp per row: hash accumulate, compact the table in place,
+// bitonic-sort the occupied entries, write the sorted row to the temporary
+// buffer at toff[i] and its length to c_cnt[i]. A row that turns out to have
+// more distinct columns than 4/5 of the table is pushed to the mid list (span
+// within mid_cols) or the largest block list and redone there.
+template <int LOG2T, int MODE>
 __global__ void __launch_bounds__(SW_THREADS)
-k_sym_warp(Operands op, const int* __restrict__ rows, int nrows, int* __restrict__ c_cnt,
-           unsigned* status) {
+k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
+             const int2* __restrict__ row_span, const long long* __restrict__ toff,
+             int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
+             int* __restrict__ mid_rows, int* __restrict__ mid_count,
+             int* __restrict__ big_rows, int* __restrict__ big_count, int mid_cols,
+             int* __restrict__ overflow_count) {
   constexpr int T = 1 << LOG2T;
+  constexpr int LIMIT = T * 4 / 5;
   constexpr int WPB = SW_THREADS / 32;
+  using V = typename SlotOf<MODE>::T;
   extern __shared__ __align__(16) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned* keys = reinterpret_cast<unsigned*>(smem) + warp * T;
-  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * 4) + warp;
+  V* vals = reinterpret_cast<V*>(smem) + warp * T;
+  unsigned* keys = reinterpret_cast<unsigned*>(smem + WPB * T * sizeof(V)) + warp * T;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * (sizeof(V) + 4)) + warp;
   for (int r = blockIdx.x * WPB + warp; r < nrows; r += gridDim.x * WPB) {
     const int i = rows[r];
-    for (int t = lane; t < T; t += 32) keys[t] = EMPTY_KEY;
+    for (int t = lane; t < T; t += 32) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
+    if (lane == 0) sc->count = 0;
     __syncwarp();
-    SymHash f{keys, LOG2T, status, 0};
-    warp_expand_row<false>(op, op.a_rowptr[i], op.a_rowptr[i + 1], f, sc);
-    const int u = warp_sum(f.nnew);
-    if (lane == 0) c_cnt[i] = u;
+    FusedHash<MODE> f{keys, vals, LOG2T, &sc->count, LIMIT};
+    warp_expand_row<true>(op, op.a_rowptr[i], op.a_rowptr[i + 1], f, sc, LIMIT);
+    __syncwarp();
+    const int distinct = *((volatile int*)&sc->count);
+    __syncwarp();
+    if (distinct > LIMIT) {  // redo with a larger structure
+      if (lane == 0) {
+        const int2 sp = row_span[i];
+        if (sp.y + 1 - (sp.x & ~31) <= mid_cols) mid_rows[atomicAdd(mid_count, 1)] = i;
+        else big_rows[atomicAdd(big_count, 1)] = i;
+        atomicAdd(overflow_count, 1);
+      }
+      continue;
+    }
+    // compact in place: entries move to lower slots only, after the whole
+    // 32-slot group has been read
+    int o = 0;
+    for (int g = 0; g < T; g += 32) {
+      const unsigned k = keys[g + lane];
+      const V v = vals[g + lane];
+      const bool valid = k != EMPTY_KEY;
+      const unsigned bal = __ballot_sync(FULL, valid);
+      const int pos = o + __popc(bal & ((1u << lane) - 1u));
+      __syncwarp();
+      if (valid) { keys[pos] = k; vals[pos] = v; }
+      o += __popc(bal);
+      __syncwarp();
+    }
+    int n2 = 1;
+    while (n2 < o) n2 <<= 1;
+    for (int t = o + lane; t < n2; t += 32) keys[t] = EMPTY_KEY;
+    __syncwarp();
+    bitonic_sort_kv_rt(keys, vals, n2, lane, 32, WarpSync());
+    const long long base = toff[i];
+    for (int t = lane; t < o; t += 32) {
+      t_col[base + t] = (int)keys[t];
+      if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+      else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    }
+    if (lane == 0) c_cnt[i] = o;
     __syncwarp();
   }
 }
 
-
-template <int LOG2T, int NT>
+// Fused pass, one block per row (rows whose column bound needs more than a
+// warp's table and whose span is too wide for the bitmap): hash accumulate
+// into 2^LOG2T slots (load <= 1/2), block compaction, bitonic sort, write the
+// sorted row to the temporary buffer. The row list may grow while earlier
+// kernels run (warp overflow), so its length is read from device memory.
+template <int LOG2T, int NT, int MODE>
 __global__ void __launch_bounds__(NT)
-k_sym_block(Operands op, const int* __restrict__ rows, int nrows,
-            const long long* __restrict__ row_p, int* __restrict__ c_cnt,
-            unsigned* status) {
+k_fused_block(Operands op, const int* __restrict__ rows, const int* __restrict__ nrows_p,
+              const long long* __restrict__ row_p, const long long* __restrict__ toff,
+              int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
+              unsigned* status) {
   constexpr int T = 1 << LOG2T;
   constexpr int NW = NT / 32;
+  constexpr int PER = T / NT;  // slots per thread in the compaction
+  using V = typename SlotOf<MODE>::T;
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int total;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  unsigned* keys = reinterpret_cast<unsigned*>(smem);
-  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * 4) + warp;
+  __shared__ long long scan_shm[33];
+  const int warp = threadIdx.x >> 5;
+  V* vals = reinterpret_cast<V*>(smem);
+  unsigned* keys = reinterpret_cast<unsigned*>(smem + T * sizeof(V));
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * (sizeof(V) + 4)) + warp;
+  const int nrows = *nrows_p;
   for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = rows[r];
-    const int p = (int)row_p[i];
-    for (int t = threadIdx.x; t < T; t += NT) keys[t] = EMPTY_KEY;
-    if (threadIdx.x == 0) total = 0;
+    const long long p = row_p[i];
+    for (int t = threadIdx.x; t < T; t += NT) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
     __syncthreads();
-    SymHash f{keys, LOG2T, status, 0};
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     const int U = chunk_for(p, NW, 1 << 20);
-    for (int c0 = warp * U; c0 < p; c0 += NW * U)
-      warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
-    const int u = warp_sum(f.nnew);
-    if (lane == 0 && u) atomicAdd(&total, u);
+    if (MODE == 0) {
+      NumHashPlain f{keys, reinterpret_cast<float*>(vals), LOG2T, status};
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + U, p), f, sc);
+    } else {
+      NumHashTwoSum f{keys, reinterpret_cast<float2*>(vals), LOG2T, status};
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, (int)min((long long)c0 + U, p), f, sc);
+    }
     __syncthreads();
-    if (threadIdx.x == 0) c_cnt[i] = total;
+    // compaction: read my PER slots, scan the counts, write after a barrier
+    unsigned k[PER];
+    V v[PER];
+    int mine = 0;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      k[q] = keys[threadIdx.x * PER + q];
+      v[q] = vals[threadIdx.x * PER + q];
+      mine += k[q] != EMPTY_KEY;
+    }
+    long long o64;
+    long long pos = block_excl_scan64(mine, scan_shm, o64);
+    const int o = (int)o64;
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+      if (k[q] != EMPTY_KEY) { keys[pos] = k[q]; vals[pos] = v[q]; ++pos; }
+    __syncthreads();
+    int n2 = 1;
+    while (n2 < o) n2 <<= 1;
+    for (int t = o + threadIdx.x; t < n2; t += NT) keys[t] = EMPTY_KEY;
+    __syncthreads();
+    bitonic_sort_kv_rt(keys, vals, n2, threadIdx.x, NT, BlockSync());
+    const long long base = toff[i];
+    for (int t = threadIdx.x; t < o; t += NT) {
+      t_col[base + t] = (int)keys[t];
+      if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+      else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    }
+    if (threadIdx.x == 0) c_cnt[i] = o;
     __syncthreads();
   }
 }
@@ -391,6 +498,27 @@ __global__ void k_rowptr_i64_to_i32_shift(const long long* __restrict__ in, int 
   }
 }
 
+// Rows finished by the fused pass: copy each row's sorted entries from the
+// temporary buffer (slot toff[i], c_cnt[i] entries) to its place in C. One
+// warp per row; rows with tcap == 0 (empty or long) are skipped.
+__global__ void __launch_bounds__(256)
+k_copy_fused(int m, const int* __restrict__ tcap, const long long* __restrict__ toff,
+             const int* __restrict__ c_cnt, const long long* __restrict__ c_rowptr,
+             const int* __restrict__ t_col, const float* __restrict__ t_val,
+             int* __restrict__ c_col, float* __restrict__ c_val) {
+  const int lane = threadIdx.x & 31;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m;
+       i += (gridDim.x * blockDim.x) >> 5) {
+    if (tcap[i] == 0) continue;
+    const int n = c_cnt[i];
+    const long long src = toff[i], dst = c_rowptr[i];
+    for (int t = lane; t < n; t += 32) {
+      __stcs(c_col + dst + t, __ldcs(t_col + src + t));
+      __stcs(c_val + dst + t, __ldcs(t_val + src + t));
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Numeric binning + long-row slicing
 // ---------------------------------------------------------------------------
@@ -404,13 +532,14 @@ __device__ __forceinline__ void push_slice(Slice* list, int* count, int capacity
   else atomicOr(status, ST_SLICE_OVERFLOW);
 }
 
-// Numeric binning. Rows whose outputs fit one block's shared memory and whose
-// column span is narrow enough get one bitmap slice covering the span:
-// "long" rows (nnz_i > long_o_num) in the big-slice list, "mid" rows
-// (mid_o_min < nnz_i <= long_o_num) in the mid-slice list. Long rows that do
-// not fit are cut into column slices from the symbolic pass's per-chunk
-// counts. The rest go to the hash bins. `bits_kept`: the symbolic pass kept
-// the bitmaps of its long rows (P_i > long_p_sym).
+// Numeric binning of the long rows (P_i > long_p; every other row was
+// finished by the fused pass). Rows whose outputs fit one block's shared
+// memory and whose column span is narrow enough get one bitmap slice
+// covering the span: rows with nnz_i > long_o_num in the big-slice list,
+// rows with mid_o_min < nnz_i <= long_o_num in the mid-slice list. Rows that
+// do not fit are cut into column slices from the symbolic pass's per-chunk
+// counts. The rest go to the block hash bins. `bits_kept`: the symbolic pass
+// kept the long rows' bitmaps.
 __global__ void __launch_bounds__(NBIN_THREADS)
 k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restrict__ row_p,
           const long long* __restrict__ c_rowptr, const int2* __restrict__ row_span,
@@ -425,7 +554,7 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
   __syncthreads();
   int bin = -1, rank = 0;
   bool listed = false;  // bitmap rows go to a slice list, not a row list
-  if (i < m) {
+  if (i < m && row_p[i] > tn.long_p) {  // other rows were done by the fused pass
     const int o = c_cnt[i];
     const long long p = row_p[i];
     bin = num_bin_of(o, p, tn);
@@ -433,7 +562,7 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
     const int lo = sp.x & ~31;  // word aligned (saved bitmaps are indexed from column 0)
     const int span = sp.y + 1 - lo;
     const long long out0 = c_rowptr[i];
-    const int flags = SLICE_WHOLE | ((bits_kept && p > tn.long_p_sym) ? SLICE_BITS_KEPT : 0);
+    const int flags = SLICE_WHOLE | (bits_kept ? SLICE_BITS_KEPT : 0);
     if (bin == NB_LONG) {
       atomicAdd(&hist[NB_LONG], 1);
       if (o <= tn.slice_cap && span <= tn.slice_cols) {
@@ -479,51 +608,6 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
 // ---------------------------------------------------------------------------
 // Numeric pass: hash rows
 // ---------------------------------------------------------------------------
-
-// Value slot type of each precision mode (0 plain, 1 compensated).
-template <int MODE> struct SlotOf { using T = float; };
-template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or double bits
-
-template <int LOG2T, int MODE>
-__global__ void __launch_bounds__(SW_THREADS)
-k_num_warp(Operands op, const int* __restrict__ rows, int nrows,
-           const long long* __restrict__ c_rowptr, int* __restrict__ c_col,
-           float* __restrict__ c_val, unsigned* status) {
-  constexpr int T = 1 << LOG2T;
-  constexpr int WPB = SW_THREADS / 32;
-  using V = typename SlotOf<MODE>::T;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  V* vals = reinterpret_cast<V*>(smem) + warp * T;
-  unsigned* keys = reinterpret_cast<unsigned*>(smem + WPB * T * sizeof(V)) + warp * T;
-  SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * (sizeof(V) + 4)) + warp;
-  for (int r = blockIdx.x * WPB + warp; r < nrows; r += gridDim.x * WPB) {
-    const int i = rows[r];
-    for (int t = lane; t < T; t += 32) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
-    __syncwarp();
-    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
-    if (MODE == 0) {
-      NumHashPlain f{keys, reinterpret_cast<float*>(vals), LOG2T, status};
-      warp_expand_row<true>(op, rs, re, f, sc);
-    } else {
-      // warp rows have P_i <= warp_p_max_num <= 4096: TwoSum, no FP64
-      NumHashTwoSum f{keys, reinterpret_cast<float2*>(vals), LOG2T, status};
-      warp_expand_row<true>(op, rs, re, f, sc);
-    }
-    __syncwarp();
-    bitonic_sort_kv<T, 32>(keys, vals, lane, WarpSync());
-    const long long o = c_rowptr[i];
-    const int cnt = (int)(c_rowptr[i + 1] - o);
-    if (lane == 0 && ((cnt < T && keys[cnt] != EMPTY_KEY) || keys[cnt - 1] == EMPTY_KEY))
-      atomicOr(status, ST_COUNT_MISMATCH);
-    for (int t = lane; t < cnt; t += 32) {
-      __stcs(c_col + o + t, (int)keys[t]);
-      if (MODE == 0) __stcs(c_val + o + t, finalize_value(reinterpret_cast<float*>(vals)[t]));
-      else __stcs(c_val + o + t, finalize_value(reinterpret_cast<float2*>(vals)[t]));
-    }
-    __syncwarp();
-  }
-}
 
 template <int LOG2T, int NT, int MODE>
 __global__ void __launch_bounds__(NT)
@@ -593,6 +677,12 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 // ranks, write-out and cleanup visit only the directory words that became
 // non-empty (tracked in l1), so a slice costs O(products + outputs) instead
 // of O(span / 32).
+//
+// Fused mode (row_list != nullptr, SPARSE only): the work items are whole rows
+// of the fused pass; the slice spans the row's columns, the output goes to the
+// temporary buffer at toff[i], the row's nnz is found here (written to
+// c_cnt[i]) and, in compensated mode, rows of at most 4096 products use
+// TwoSum pairs instead of FP64.
 template <int MODE, int NT, bool SPARSE>
 __global__ void __launch_bounds__(NT)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
@@ -600,7 +690,10 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            int* __restrict__ scratch, int scratch_stride,
            const unsigned* __restrict__ bitmaps, int bitmap_words,
            const int* __restrict__ long_slot,
-           int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
+           int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status,
+           const int* __restrict__ row_list, const int* __restrict__ row_count_p,
+           const int2* __restrict__ row_span, const long long* __restrict__ toff,
+           int* __restrict__ c_cnt) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long scan_shm[33];
@@ -617,15 +710,24 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     for (int t = threadIdx.x; t < dir_words; t += NT) dir[t] = make_uint2(0u, 0u);
     for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
   }
+  if (row_list) nslices = *row_count_p;
   for (int s = blockIdx.x; s < nslices; s += gridDim.x) {
-    const Slice sl = slices[s];
+    Slice sl;
+    if (row_list) {
+      const int ri = row_list[s];
+      const int2 sp = row_span[ri];
+      sl = Slice{toff[ri], ri, sp.x & ~31, sp.y + 1, -1, SLICE_WHOLE | SLICE_FUSED};
+    } else {
+      sl = slices[s];
+    }
     const int i = sl.row;
+    const bool fused = (sl.flags & SLICE_FUSED) != 0;
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     int* roff = seg_start + (re - rs);
     const bool whole = (sl.flags & SLICE_WHOLE) != 0;
     const int nw = (sl.hi - sl.lo + 31) >> 5;
     const int cnt = sl.cnt;
-    if (nw > dir_words || cnt > cap || (SPARSE && !whole)) {  // host sizing prevents this
+    if (nw > dir_words || cnt > cap || (SPARSE && !whole)) {  // sizing prevents this
       if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
       continue;
     }
@@ -708,7 +810,8 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       for (int q = 0; q < per; ++q)
         if (w0 + q < nw) { dir[w0 + q].y = (unsigned)run; run += __popc(dir[w0 + q].x); }
     }
-    if (tot != cnt || (SPARSE && nt == cap && cnt < cap)) {  // block-uniform
+    const int ocount = fused ? (int)tot : cnt;
+    if ((!fused && tot != cnt) || tot > cap || (SPARSE && nt == cap && ocount < cap)) {  // block-uniform
       if (threadIdx.x == 0) atomicOr(status, ST_COUNT_MISMATCH);
       __syncthreads();
       if (SPARSE) {  // restore the clean directory before the next slice
@@ -720,14 +823,21 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     }
     if (MODE == 0) {
       float* vals = reinterpret_cast<float*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += NT) vals[t] = 0.f;
+      for (int t = threadIdx.x; t < ocount; t += NT) vals[t] = 0.f;
     } else {
-      double* vals = reinterpret_cast<double*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += NT) vals[t] = 0.0;
+      double* vals = reinterpret_cast<double*>(vbase);  // zero bits: 0.0 and (0.f, 0.f)
+      for (int t = threadIdx.x; t < ocount; t += NT) vals[t] = 0.0;
     }
     __syncthreads();
+    const bool pair = MODE == 1 && p <= FP64_ROW_PARTIALS;  // compensated FP32 pairs
     // value pass
-    if (MODE == 0) {
+    if (MODE == 1 && pair) {
+      LongValTwoSum f{dir, reinterpret_cast<float2*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
+        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
+      }
+    } else if (MODE == 0) {
       LongValPlain f{dir, reinterpret_cast<float*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
         if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
@@ -743,12 +853,16 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     __syncthreads();
     // write-out: values are already in output order (coalesced copy);
     // columns are expanded word by word from the bitmap
+    if (fused && threadIdx.x == 0) c_cnt[i] = ocount;
     if (MODE == 0) {
       const float* vals = reinterpret_cast<const float*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += NT) __stcs(c_val + sl.out + t, vals[t]);
+      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, vals[t]);
+    } else if (pair) {
+      const float2* vals = reinterpret_cast<const float2*>(vbase);
+      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
     } else {
       const double* vals = reinterpret_cast<const double*>(vbase);
-      for (int t = threadIdx.x; t < cnt; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
+      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
     }
     if (SPARSE) {
       for (int t = threadIdx.x; t < nt; t += NT) {

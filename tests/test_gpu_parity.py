@@ -85,8 +85,9 @@ def test_empty_product():
 def test_rmat_all_bins():
     A = W.rmat(14, 16, 1)
     _, _, stats = check(A, A)
-    assert stats["rows_per_symbolic_bin"][8] > 0, stats
-    assert stats["rows_per_numeric_bin"][8] > 0, stats
+    assert stats["rows_per_symbolic_bin"][9] > 0, stats   # long rows
+    assert stats["rows_per_symbolic_bin"][8] > 0, stats   # fused span bitmap
+    assert stats["rows_per_numeric_bin"][8] > 0, stats    # column slices
 
 
 def test_rmat_all_bins_compensated():
@@ -154,12 +155,14 @@ def test_repeat_calls_reuse_workspace():
 TUNINGS = [
     dict(keep_bitmaps=0),                                   # numeric rebuilds long-row bitmaps
     dict(slice_cap=2048, slice_cols=8192),                  # many column slices per long row
-    dict(warp_p_max_sym=0, warp_p_max_num=0),               # every short row block-per-row
-    dict(long_p_sym=256, long_o_num=256),                   # mid rows take the long path
+    dict(warp_p_max=0),                                     # no fused warp rows: block / bitmap
+    dict(warp_table_max=64),                                # most warp rows overflow and are redone
+    dict(warp_table_max=1024, warp_cap_max=4096),           # large warp tables
+    dict(long_p=256, long_o_num=256),                       # mid rows take the two-pass path
+    dict(long_p=64, long_o_num=64, mid_o_min=0),            # long path + span bitmap numeric
     dict(sym_window=4096, slice_cols=4096, slice_cap=2048,  # multi-window symbolic pass,
          keep_bitmaps=0),                                   # restricted numeric slices
-    dict(mid_o_min=0),                                      # every row with outputs: bitmap kernel
-    dict(mid_cols=0),                                       # no mid bitmap rows: hash bins only
+    dict(mid_cols=0),                                       # no bitmaps: hash tables only
 ]
 
 
@@ -182,11 +185,13 @@ def test_tuning_overrides(tuning, precision):
 def test_bad_tuning_rejected():
     with sg.Handle() as h:
         with pytest.raises(sg.SpgemmError):
-            h.set_tuning(long_o_num=100, long_p_sym=200)
+            h.set_tuning(long_o_num=5000)
         with pytest.raises(sg.SpgemmError):
             h.set_tuning(slice_cols=1000)
         with pytest.raises(sg.SpgemmError):
-            h.set_tuning(long_p_sym=5000)
+            h.set_tuning(long_p=5000)
+        with pytest.raises(sg.SpgemmError):
+            h.set_tuning(warp_table_max=100)
 
 
 def _dev(a, dtype, offset=0):
