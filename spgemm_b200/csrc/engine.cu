@@ -552,7 +552,6 @@ size_t Engine::big_dir_bytes() const {
 
 template <int MODE>
 int Engine::launch_numeric_mode(int* c_col, float* c_val) {
-  constexpr int WPB = SW_THREADS / 32;
   constexpr int MID_THREADS = 512;
   constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
   const Operands op = op_;

@@ -158,6 +158,12 @@ __device__ __forceinline__ int compact_segments(int& bstart, int& len, float& a,
   return cnt;
 }
 
+// Loop unrolling of the product walks: windows / 128-bit groups whose loads
+// are issued before their accumulates, for passes that load values (VAL) or
+// only columns (BITS).
+constexpr int WIN_UNROLL_VAL = 2, WIN_UNROLL_BITS = 4;
+constexpr int VEC_UNROLL_VAL = 2, VEC_UNROLL_BITS = 4;
+
 // Generate every partial product of the (<= 32) compacted segments held by
 // the warp: lane j < cnt holds B positions [bstart, bstart + len) to be
 // scaled by a. The segments are laid end to end and walked 32 products at a
@@ -174,7 +180,7 @@ template <bool NEED_VAL, class F>
 __device__ __forceinline__ void run_segments(int cnt, int bstart, int len, float a,
                                              const int* __restrict__ b_col,
                                              const float* __restrict__ b_val, F& f) {
-  constexpr int UNROLL = 4;  // windows whose loads are issued before their accumulates
+  constexpr int UNROLL = NEED_VAL ? WIN_UNROLL_VAL : WIN_UNROLL_BITS;  // windows in flight
   const int lane = lane_id();
   if (lane >= cnt) len = 0;
   const int incl = warp_incl_scan(len);
@@ -239,7 +245,7 @@ __device__ __forceinline__ void warp_run_segment_vec(int bs, int len, float a,
   const int n4 = (end - body0) >> 2;
   const int4* c4 = reinterpret_cast<const int4*>(b_col + body0);
   const float4* v4 = reinterpret_cast<const float4*>(b_val + body0);
-  constexpr int VU = 4;  // groups of 4 products whose loads are in flight together
+  constexpr int VU = NEED_VAL ? VEC_UNROLL_VAL : VEC_UNROLL_BITS;  // groups in flight together
   int g = lane;
   for (; g + 32 * (VU - 1) < n4; g += 32 * VU) {
     int4 c[VU];

@@ -190,7 +190,7 @@ template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or do
 // more distinct columns than 4/5 of the table is pushed to the mid list (span
 // within mid_cols) or the largest block list and redone there.
 template <int LOG2T, int MODE>
-__global__ void __launch_bounds__(SW_THREADS)
+__global__ void __launch_bounds__(SW_THREADS, 4)
 k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
              const int2* __restrict__ row_span, const long long* __restrict__ toff,
              int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
@@ -261,7 +261,7 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
 // sorted row to the temporary buffer. The row list may grow while earlier
 // kernels run (warp overflow), so its length is read from device memory.
 template <int LOG2T, int NT, int MODE>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 4)
 k_fused_block(Operands op, const int* __restrict__ rows, const int* __restrict__ nrows_p,
               const long long* __restrict__ row_p, const long long* __restrict__ toff,
               int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
@@ -332,7 +332,7 @@ constexpr int LONG_THREADS = 1024;
 // Exact nnz of long rows: presence bitmap of the row's columns in shared
 // memory, one window of `tn.sym_window` columns at a time. Also records the
 // nnz of every 2048-column chunk, from which k_num_bin cuts column slices.
-__global__ void __launch_bounds__(LONG_THREADS)
+__global__ void __launch_bounds__(LONG_THREADS, 2)
 k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
            const long long* __restrict__ row_p, int* __restrict__ c_cnt,
            int* __restrict__ long_slot, int* __restrict__ chunk_cnt, int n_chunks,
@@ -683,8 +683,114 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 // temporary buffer at toff[i], the row's nnz is found here (written to
 // c_cnt[i]) and, in compensated mode, rows of at most 4096 products use
 // TwoSum pairs instead of FP64.
+// Directory walks shared by the rank scan and the column write-out: list
+// item t names directory word word_at(t); each warp takes one contiguous run
+// of the list (a multiple of 32 items) and walks it 32 items at a time, lane
+// l on item base + l, so shared-memory accesses are conflict-free and the
+// ranks, hence the output positions, rise with the lane.
+template <int NT>
+__device__ __forceinline__ int2 warp_dir_run(int nitems) {
+  constexpr int NW = NT / 32;
+  const int run = ((nitems + NW * 32 - 1) / (NW * 32)) * 32;
+  const int b = min((int)(threadIdx.x >> 5) * run, nitems);
+  return make_int2(b, min(b + run, nitems));
+}
+
+// Ranks of a bitmap directory: dir[w].y = set bits in the listed words before
+// w. Returns the total number of set bits (every thread). The ranks are
+// visible to the whole block after the caller's next barrier.
+template <int NT, class WordAt>
+__device__ __forceinline__ long long dir_ranks(uint2* dir, int nitems, WordAt word_at,
+                                               long long* scan_shm) {
+  const int lane = lane_id();
+  const int2 r = warp_dir_run<NT>(nitems);
+  int local = 0;
+  for (int t = r.x + lane; t < r.y; t += 32) local += __popc(dir[word_at(t)].x);
+  local = warp_sum(local);
+  long long total;
+  long long base = block_excl_scan64(lane == 0 ? local : 0, scan_shm, total);
+  base = __shfl_sync(FULL, base, 0);
+  for (int t0 = r.x; t0 < r.y; t0 += 32) {
+    const int t = t0 + lane;
+    const int w = t < r.y ? word_at(t) : 0;
+    const int c = t < r.y ? __popc(dir[w].x) : 0;
+    const int incl = warp_incl_scan(c);
+    if (t < r.y) dir[w].y = (unsigned)(base + incl - c);
+    base += __shfl_sync(FULL, incl, 31);
+  }
+  return total;
+}
+
+// First list item t in [0, n) whose key is >= target (n if none), for keys
+// that do not decrease with t; the whole warp searches, 32 probes per step.
+template <class Key>
+__device__ __forceinline__ int warp_lower_bound(int n, long long target, Key key) {
+  const int lane = lane_id();
+  int lo = 0, hi = n;  // the answer lies in [lo, hi]
+  while (lo < hi) {
+    const int step = (hi - lo + 31) >> 5;
+    const int t = lo + (lane + 1) * step - 1;
+    const bool ge = t >= hi || (long long)key(t) >= target;
+    const unsigned m = __ballot_sync(FULL, ge);
+    if (m == 0) return hi;  // every probe below target: probe 31 is hi - 1
+    const int f = __ffs(m) - 1;
+    const int nlo = lo + f * step;
+    hi = min(hi, nlo + step - 1);
+    lo = nlo;
+  }
+  return lo;
+}
+
+// Words with at least this many columns are written by the whole warp.
+constexpr int DENSE_WORD_BITS = 6;
+
+// Column indices of a slice from its ranked directory: the columns of word w
+// (lo + 32 w + bit) go to c_col[out + dir[w].y ...] in bit order. The list is
+// split between the warps by output count (warp k takes the words whose rank
+// falls in its 1/NW share of `total`), so a run of dense words -- the popular
+// columns of a power-law matrix -- does not hold one warp while the others
+// wait at the next barrier. A word with few bits is written by its own lane
+// (the lanes' ranks are adjacent, so the stores of a warp stay within a few
+// lines); a word with many bits by the whole warp, one bit per lane, in a
+// single coalesced store.
+template <int NT, class WordAt>
+__device__ __forceinline__ void dir_write_cols(const uint2* dir, int nitems, WordAt word_at,
+                                               long long total, int lo, long long out,
+                                               int* __restrict__ c_col) {
+  constexpr int NW = NT / 32;
+  const int lane = lane_id(), warp = threadIdx.x >> 5;
+  const unsigned below = (1u << lane) - 1u;
+  auto rank_at = [&](int t) { return dir[word_at(t)].y; };
+  const int wb = warp == 0 ? 0 : warp_lower_bound(nitems, total * warp / NW, rank_at);
+  const int we = warp == NW - 1 ? nitems : warp_lower_bound(nitems, total * (warp + 1) / NW, rank_at);
+  for (int t0 = wb; t0 < we; t0 += 32) {
+    const int t = t0 + lane;
+    uint2 d = make_uint2(0u, 0u);
+    int w = 0;
+    if (t < we) { w = word_at(t); d = dir[w]; }
+    const int cbase = lo + w * 32;
+    const bool dense = __popc(d.x) >= DENSE_WORD_BITS;
+    unsigned dm = __ballot_sync(FULL, dense);
+    unsigned bits = dense ? 0u : d.x;
+    long long o = out + d.y;
+    while (bits) {
+      __stcs(c_col + o++, cbase + __ffs(bits) - 1);
+      bits &= bits - 1u;
+    }
+    __syncwarp();
+    while (dm) {
+      const int src = __ffs(dm) - 1;
+      dm &= dm - 1u;
+      const unsigned b = __shfl_sync(FULL, d.x, src);
+      const unsigned rk = __shfl_sync(FULL, d.y, src);
+      const int cb = __shfl_sync(FULL, cbase, src);
+      if ((b >> lane) & 1u) __stcs(c_col + out + rk + __popc(b & below), cb + lane);
+    }
+  }
+}
+
 template <int MODE, int NT, bool SPARSE>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 2)
 k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            const long long* __restrict__ row_p, int dir_words, int cap,
            int* __restrict__ scratch, int scratch_stride,
@@ -788,27 +894,9 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       }
       nt = (int)min(l1tot, (long long)cap);  // more than cap touched words: count mismatch below
       __syncthreads();
-      const int per = (nt + NT - 1) / NT;
-      const int t0 = threadIdx.x * per;
-      int local = 0;
-      for (int q = 0; q < per; ++q)
-        if (t0 + q < nt) local += __popc(dir[touched[t0 + q]].x);
-      long long run = block_excl_scan64(local, scan_shm, tot);
-      for (int q = 0; q < per; ++q)
-        if (t0 + q < nt) {
-          uint2& d = dir[touched[t0 + q]];
-          d.y = (unsigned)run;
-          run += __popc(d.x);
-        }
+      tot = dir_ranks<NT>(dir, nt, [&](int t) { return touched[t]; }, scan_shm);
     } else {
-      const int per = (nw + NT - 1) / NT;
-      const int w0 = threadIdx.x * per;
-      int local = 0;
-      for (int q = 0; q < per; ++q)
-        if (w0 + q < nw) local += __popc(dir[w0 + q].x);
-      long long run = block_excl_scan64(local, scan_shm, tot);
-      for (int q = 0; q < per; ++q)
-        if (w0 + q < nw) { dir[w0 + q].y = (unsigned)run; run += __popc(dir[w0 + q].x); }
+      tot = dir_ranks<NT>(dir, nw, [](int t) { return t; }, scan_shm);
     }
     const int ocount = fused ? (int)tot : cnt;
     if ((!fused && tot != cnt) || tot > cap || (SPARSE && nt == cap && ocount < cap)) {  // block-uniform
@@ -865,30 +953,13 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
     }
     if (SPARSE) {
-      for (int t = threadIdx.x; t < nt; t += NT) {
-        const int w = touched[t];
-        unsigned bits = dir[w].x;
-        long long o = sl.out + dir[w].y;
-        const int cbase = sl.lo + w * 32;
-        while (bits) {
-          __stcs(c_col + o++, cbase + __ffs(bits) - 1);
-          bits &= bits - 1u;
-        }
-      }
+      dir_write_cols<NT>(dir, nt, [&](int t) { return touched[t]; }, ocount, sl.lo, sl.out, c_col);
       __syncthreads();
       // leave the directory clean for the next slice
       for (int t = threadIdx.x; t < nt; t += NT) dir[touched[t]] = make_uint2(0u, 0u);
       for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
     } else {
-      for (int w = threadIdx.x; w < nw; w += NT) {
-        unsigned bits = dir[w].x;
-        long long o = sl.out + dir[w].y;
-        const int cbase = sl.lo + w * 32;
-        while (bits) {
-          __stcs(c_col + o++, cbase + __ffs(bits) - 1);
-          bits &= bits - 1u;
-        }
-      }
+      dir_write_cols<NT>(dir, nw, [](int t) { return t; }, ocount, sl.lo, sl.out, c_col);
     }
     __syncthreads();
   }
