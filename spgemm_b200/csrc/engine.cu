@@ -50,8 +50,11 @@ Tuning default_tuning() {
   return t;
 }
 
-// Dynamic shared memory available to one long-row block.
-static constexpr size_t LONG_SMEM_BUDGET = 220 * 1024;
+// Big bitmap slices of long rows: threads of one block, blocks resident per
+// SM, and the shared memory one block may use.
+static constexpr int BIG_THREADS = 1024;
+static constexpr int BIG_BLOCKS_PER_SM = 1;
+static constexpr size_t BIG_SMEM_BUDGET = 220 * 1024;
 static constexpr size_t SEG_SCRATCH_BYTES = sizeof(SegScratch);
 
 Engine::Engine() {
@@ -365,9 +368,9 @@ int Engine::symbolic_pass(long long* nnz_c) {
   // output capacity of one big slice: what the shared-memory budget leaves
   Tuning tr = tn_;
   {
-    const size_t vb = precision_ == 1 ? 8 : 4;
-    const size_t fixed = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes();
-    long long cap = (long long)((LONG_SMEM_BUDGET - fixed) / vb);
+    const size_t vb = (precision_ == 1 ? 8 : 4) + sizeof(int);  // value and column per slot
+    const size_t fixed = (BIG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes();
+    long long cap = (long long)((BIG_SMEM_BUDGET - fixed) / vb);
     cap = std::min<long long>(cap, 1 << 20);
     if (tn_.slice_cap > 0) cap = std::min<long long>(cap, tn_.slice_cap);
     tr.slice_cap = (int)cap;
@@ -484,7 +487,7 @@ int Engine::launch_fused() {
     const int dir_words = (width + 31) / 32;
     const int cap = (int)std::min<long long>(tn_.long_p, n_);
     const size_t smem = (MID_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)dir_words * sizeof(uint2) +
-                        (size_t)cap * 8 + sizeof(unsigned) * ((dir_words + 31) / 32) +
+                        (size_t)cap * (8 + sizeof(int)) + sizeof(unsigned) * ((dir_words + 31) / 32) +
                         sizeof(int) * (size_t)cap;
     SG_CK(smem_attr(k_num_long<MODE, MID_THREADS, true>, smem), "smem attr k_num_long fused");
     const int grid = blocks_for(fb_counts_[FB_MID] + overflow_bound, 1, (long long)sms_ * 4);
@@ -561,16 +564,16 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   const long long* c_rowptr = c_rowptr64_.as<long long>();
   unsigned* status = &counters_.as<DevCounters>()->status;
   const int stride = 2 * max_row_len_ + 2;
-  // big bitmap slices (long rows), one 1024-thread block per SM
+  // big bitmap slices (long rows)
   if (nslices_ > 0) {
     const int dir_words = (int)(big_dir_bytes() / sizeof(uint2));
-    const size_t smem = (LONG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes() +
-                        (size_t)tn_run_slice_cap_ * (MODE ? 8 : 4);
-    SG_CK(smem_attr(k_num_long<MODE, LONG_THREADS, false>, smem), "smem attr k_num_long");
-    const int grid = blocks_for(nslices_, 1, (long long)sms_ * 2);
+    const size_t smem = (BIG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes() +
+                        (size_t)tn_run_slice_cap_ * ((MODE ? 8 : 4) + sizeof(int));
+    SG_CK(smem_attr(k_num_long<MODE, BIG_THREADS, false>, smem), "smem attr k_num_long");
+    const int grid = blocks_for(nslices_, 1, (long long)sms_ * BIG_BLOCKS_PER_SM * 2);
     SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
     prof_begin("k_num_long");
-    k_num_long<MODE, LONG_THREADS, false><<<grid, LONG_THREADS, smem, stream_>>>(
+    k_num_long<MODE, BIG_THREADS, false><<<grid, BIG_THREADS, smem, stream_>>>(
         op, slices_buf_.as<Slice>(), nslices_, row_p, dir_words, tn_run_slice_cap_,
         restrict_scratch_.as<int>(), stride, bitmaps_.as<unsigned>(), bitmap_words_,
         long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr);
@@ -582,8 +585,8 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     const int dir_words = (width + 31) / 32;            // <= 8193, so l1 fits 512 threads
     const int cap = tn_.long_o_num;
     const size_t smem = (MID_THREADS / 32) * SEG_SCRATCH_BYTES + (size_t)dir_words * sizeof(uint2) +
-                        (size_t)cap * (MODE ? 8 : 4) + sizeof(unsigned) * ((dir_words + 31) / 32) +
-                        sizeof(int) * (size_t)cap;
+                        (size_t)cap * ((MODE ? 8 : 4) + sizeof(int)) +
+                        sizeof(unsigned) * ((dir_words + 31) / 32) + sizeof(int) * (size_t)cap;
     SG_CK(smem_attr(k_num_long<MODE, MID_THREADS, true>, smem), "smem attr k_num_long mid");
     const int grid = blocks_for(nmid_, 1, (long long)sms_ * 4);
     prof_begin("k_num_mid");

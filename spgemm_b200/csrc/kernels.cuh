@@ -679,6 +679,7 @@ __device__ __forceinline__ void bitonic_sort_kv_rt(unsigned* keys, V* vals, int 
 struct LongValTwoSum {
   const uint2* dir;
   float2* vals;
+  int* cols;
   int lo;
   unsigned width;
   __device__ __forceinline__ void operator()(int col, float a, float b);
@@ -712,28 +713,45 @@ __device__ __forceinline__ int long_slot(const uint2* dir, int lo, int col) {
   return (int)(d.y + __popc(d.x & ((1u << (c & 31)) - 1u)));
 }
 
+// Value-pass functors of the bitmap slices: accumulate into the output slot
+// and record the slot's column (every product of a column stores the same
+// index), so the write-out copies columns like values instead of expanding
+// the directory.
 struct LongValPlain {
   const uint2* dir;
   float* vals;
+  int* cols;
   int lo;
   unsigned width;
   __device__ __forceinline__ void operator()(int col, float a, float b) {
-    if ((unsigned)(col - lo) < width) atomicAdd(vals + long_slot(dir, lo, col), __fmul_rn(a, b));
+    if ((unsigned)(col - lo) < width) {
+      const int s = long_slot(dir, lo, col);
+      atomicAdd(vals + s, __fmul_rn(a, b));
+      cols[s] = col;
+    }
   }
 };
 
 __device__ __forceinline__ void LongValTwoSum::operator()(int col, float a, float b) {
-  if ((unsigned)(col - lo) < width) twosum_accumulate(vals + long_slot(dir, lo, col), a, b);
+  if ((unsigned)(col - lo) < width) {
+    const int s = long_slot(dir, lo, col);
+    twosum_accumulate(vals + s, a, b);
+    cols[s] = col;
+  }
 }
 
 struct LongValF64 {
   const uint2* dir;
   double* vals;
+  int* cols;
   int lo;
   unsigned width;
   __device__ __forceinline__ void operator()(int col, float a, float b) {
-    if ((unsigned)(col - lo) < width)
-      atomicAdd(vals + long_slot(dir, lo, col), (double)a * (double)b);
+    if ((unsigned)(col - lo) < width) {
+      const int s = long_slot(dir, lo, col);
+      atomicAdd(vals + s, (double)a * (double)b);
+      cols[s] = col;
+    }
   }
 };
 

@@ -721,72 +721,14 @@ __device__ __forceinline__ long long dir_ranks(uint2* dir, int nitems, WordAt wo
   return total;
 }
 
-// First list item t in [0, n) whose key is >= target (n if none), for keys
-// that do not decrease with t; the whole warp searches, 32 probes per step.
-template <class Key>
-__device__ __forceinline__ int warp_lower_bound(int n, long long target, Key key) {
-  const int lane = lane_id();
-  int lo = 0, hi = n;  // the answer lies in [lo, hi]
-  while (lo < hi) {
-    const int step = (hi - lo + 31) >> 5;
-    const int t = lo + (lane + 1) * step - 1;
-    const bool ge = t >= hi || (long long)key(t) >= target;
-    const unsigned m = __ballot_sync(FULL, ge);
-    if (m == 0) return hi;  // every probe below target: probe 31 is hi - 1
-    const int f = __ffs(m) - 1;
-    const int nlo = lo + f * step;
-    hi = min(hi, nlo + step - 1);
-    lo = nlo;
-  }
-  return lo;
-}
-
-// Words with at least this many columns are written by the whole warp.
-constexpr int DENSE_WORD_BITS = 6;
-
-// Column indices of a slice from its ranked directory: the columns of word w
-// (lo + 32 w + bit) go to c_col[out + dir[w].y ...] in bit order. The list is
-// split between the warps by output count (warp k takes the words whose rank
-// falls in its 1/NW share of `total`), so a run of dense words -- the popular
-// columns of a power-law matrix -- does not hold one warp while the others
-// wait at the next barrier. A word with few bits is written by its own lane
-// (the lanes' ranks are adjacent, so the stores of a warp stay within a few
-// lines); a word with many bits by the whole warp, one bit per lane, in a
-// single coalesced store.
-template <int NT, class WordAt>
-__device__ __forceinline__ void dir_write_cols(const uint2* dir, int nitems, WordAt word_at,
-                                               long long total, int lo, long long out,
-                                               int* __restrict__ c_col) {
-  constexpr int NW = NT / 32;
-  const int lane = lane_id(), warp = threadIdx.x >> 5;
-  const unsigned below = (1u << lane) - 1u;
-  auto rank_at = [&](int t) { return dir[word_at(t)].y; };
-  const int wb = warp == 0 ? 0 : warp_lower_bound(nitems, total * warp / NW, rank_at);
-  const int we = warp == NW - 1 ? nitems : warp_lower_bound(nitems, total * (warp + 1) / NW, rank_at);
-  for (int t0 = wb; t0 < we; t0 += 32) {
-    const int t = t0 + lane;
-    uint2 d = make_uint2(0u, 0u);
-    int w = 0;
-    if (t < we) { w = word_at(t); d = dir[w]; }
-    const int cbase = lo + w * 32;
-    const bool dense = __popc(d.x) >= DENSE_WORD_BITS;
-    unsigned dm = __ballot_sync(FULL, dense);
-    unsigned bits = dense ? 0u : d.x;
-    long long o = out + d.y;
-    while (bits) {
-      __stcs(c_col + o++, cbase + __ffs(bits) - 1);
-      bits &= bits - 1u;
-    }
-    __syncwarp();
-    while (dm) {
-      const int src = __ffs(dm) - 1;
-      dm &= dm - 1u;
-      const unsigned b = __shfl_sync(FULL, d.x, src);
-      const unsigned rk = __shfl_sync(FULL, d.y, src);
-      const int cb = __shfl_sync(FULL, cbase, src);
-      if ((b >> lane) & 1u) __stcs(c_col + out + rk + __popc(b & below), cb + lane);
-    }
-  }
+// dst[0, n) = f(t) for t in [0, n), by the whole block, each warp store
+// covering one aligned 128-byte line of dst (streaming stores: C is not
+// read again by this pass).
+template <int NT, class T, class F>
+__device__ __forceinline__ void block_store_aligned(T* __restrict__ dst, int n, F f) {
+  const int head = (int)((reinterpret_cast<size_t>(dst) / sizeof(T)) & (128 / sizeof(T) - 1));
+  for (int g = threadIdx.x - head; g < n; g += NT)
+    if (g >= 0) __stcs(dst + g, f(g));
 }
 
 template <int MODE, int NT, bool SPARSE>
@@ -808,8 +750,9 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
   uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
   unsigned char* vbase = smem + NW * sizeof(SegScratch) + (size_t)dir_words * sizeof(uint2);
+  int* cols = reinterpret_cast<int*>(vbase + (size_t)cap * (MODE ? 8 : 4));  // column per slot
   const int l1_words = (dir_words + 31) >> 5;
-  unsigned* l1 = reinterpret_cast<unsigned*>(vbase + (size_t)cap * (MODE ? 8 : 4));
+  unsigned* l1 = reinterpret_cast<unsigned*>(cols + cap);
   int* touched = reinterpret_cast<int*>(l1 + l1_words);
   int* seg_start = scratch + (size_t)blockIdx.x * scratch_stride;
   if (SPARSE) {
@@ -920,46 +863,42 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     const bool pair = MODE == 1 && p <= FP64_ROW_PARTIALS;  // compensated FP32 pairs
     // value pass
     if (MODE == 1 && pair) {
-      LongValTwoSum f{dir, reinterpret_cast<float2*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      LongValTwoSum f{dir, reinterpret_cast<float2*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
         if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     } else if (MODE == 0) {
-      LongValPlain f{dir, reinterpret_cast<float*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      LongValPlain f{dir, reinterpret_cast<float*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
         if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     } else {
-      LongValF64 f{dir, reinterpret_cast<double*>(vbase), sl.lo, (unsigned)(sl.hi - sl.lo)};
+      LongValF64 f{dir, reinterpret_cast<double*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
       for (int c0 = warp * U; c0 < p; c0 += NW * U) {
         if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
         else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
       }
     }
     __syncthreads();
-    // write-out: values are already in output order (coalesced copy);
-    // columns are expanded word by word from the bitmap
+    // write-out: values and columns are already in output order
     if (fused && threadIdx.x == 0) c_cnt[i] = ocount;
     if (MODE == 0) {
       const float* vals = reinterpret_cast<const float*>(vbase);
-      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, vals[t]);
+      block_store_aligned<NT>(c_val + sl.out, ocount, [&](int t) { return vals[t]; });
     } else if (pair) {
       const float2* vals = reinterpret_cast<const float2*>(vbase);
-      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
+      block_store_aligned<NT>(c_val + sl.out, ocount, [&](int t) { return finalize_value(vals[t]); });
     } else {
       const double* vals = reinterpret_cast<const double*>(vbase);
-      for (int t = threadIdx.x; t < ocount; t += NT) __stcs(c_val + sl.out + t, finalize_value(vals[t]));
+      block_store_aligned<NT>(c_val + sl.out, ocount, [&](int t) { return finalize_value(vals[t]); });
     }
+    block_store_aligned<NT>(c_col + sl.out, ocount, [&](int t) { return cols[t]; });
     if (SPARSE) {
-      dir_write_cols<NT>(dir, nt, [&](int t) { return touched[t]; }, ocount, sl.lo, sl.out, c_col);
-      __syncthreads();
       // leave the directory clean for the next slice
       for (int t = threadIdx.x; t < nt; t += NT) dir[touched[t]] = make_uint2(0u, 0u);
       for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
-    } else {
-      dir_write_cols<NT>(dir, nw, [](int t) { return t; }, ocount, sl.lo, sl.out, c_col);
     }
     __syncthreads();
   }
