@@ -141,6 +141,44 @@ int spgemm_multiply_host_to(spgemm_handle_t handle, cm A_host, cm B_host,
                             int* c_rowptr, int* c_colidx, float* c_val,
                             long long capacity, long long* nnz_c);
 
+/* Batched products. The reference multiplies one pair per process
+ * (src/main.cu:31-37 drives src/mm.cu once); these entry points run `count`
+ * independent products C_i = A_i * B_i together: the operands are packed
+ * into one block-diagonal product on the device, so each bin kernel of the
+ * pipeline serves every product in one launch.
+ *   A[i]: device CSR (every A_i) or device CSC (every A_i); B[i]: device CSR;
+ *   A[i].num_cols == B[i].num_rows; ptr[0] == 0 for every operand.
+ * spgemm_batch_plan runs the whole batch once (host-synchronised), keeps its
+ * sizes and returns the total nnz over all C_i. It replaces the handle's
+ * current product. spgemm_batch_execute recomputes every C_i from the
+ * current contents of the same operand arrays (same structure, any values)
+ * with no host synchronisation inside: with use_graph != 0 the pipeline is
+ * recorded into a CUDA graph on its first call and replayed afterwards (on
+ * the handle's stream, or a handle-owned stream when that is the default
+ * stream). It synchronises once at the end to check the device status.
+ * Any other product run on the handle invalidates the plan
+ * (SPGEMM_ERR_STATE; plan again).
+ * Output (handle-owned device memory, valid until the next plan or
+ * spgemm_destroy): spgemm_batch_result gives product i as a device cm with
+ * local row pointers (from 0) and B_i's column indices; each C_i holds at
+ * most INT32_MAX entries (else SPGEMM_ERR_OVERFLOW at plan time), the total
+ * may exceed it. spgemm_batch_offsets writes count + 1 row offsets (product
+ * i owns rows [row_off[i], row_off[i+1]) of the packed product; its row
+ * pointers start at packed position row_off[i] + i) and count + 1 entry
+ * offsets. spgemm_batch_copy_result copies product i to host arrays
+ * (rowptr[m_i + 1], colidx/val[nnz_i]); spgemm_batch_copy_all copies the
+ * whole packed output (rowptr[row_off[count] + count], colidx/val[total]). */
+int spgemm_batch_plan(spgemm_handle_t handle, int count, const cm* A, const cm* B,
+                      long long* nnz_total);
+int spgemm_batch_execute(spgemm_handle_t handle, int use_graph);
+int spgemm_batch_offsets(spgemm_handle_t handle, long long* row_offsets,
+                         long long* nnz_offsets);
+int spgemm_batch_result(spgemm_handle_t handle, int i, cm* C);
+int spgemm_batch_copy_result(spgemm_handle_t handle, int i, int* c_rowptr,
+                             int* c_colidx, float* c_val);
+int spgemm_batch_copy_all(spgemm_handle_t handle, int* c_rowptr, int* c_colidx,
+                          float* c_val);
+
 /* Per-kernel timing: when enabled, CUDA events are recorded on the handle's
  * stream around every engine kernel launch and accumulated per kernel name
  * (collected at the end of each numeric pass). */

@@ -109,6 +109,13 @@ def lib():
         L.spgemm_reset_kernel_times.argtypes = [vp]
         L.spgemm_get_kernel_times.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
+        L.spgemm_batch_plan.argtypes = [vp, C.c_int, C.POINTER(CM), C.POINTER(CM),
+                                        C.POINTER(C.c_longlong)]
+        L.spgemm_batch_execute.argtypes = [vp, C.c_int]
+        L.spgemm_batch_offsets.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.spgemm_batch_result.argtypes = [vp, C.c_int, C.POINTER(CM)]
+        L.spgemm_batch_copy_result.argtypes = [vp, C.c_int, ip, ip, fp]
+        L.spgemm_batch_copy_all.argtypes = [vp, vp, vp, vp]
         L.cmFree.argtypes = [C.POINTER(CM)]
         L.cudaCOO2CM.restype = CM
         L.cudaCOO2CM.argtypes = [COO]
@@ -192,6 +199,7 @@ class Handle:
 
     def set_precision(self, p: int):
         self._check(lib().spgemm_set_precision(self._h, p))
+        self.precision = p
 
     def set_stream(self, stream_ptr: int):
         self._check(lib().spgemm_set_stream(self._h, C.c_void_p(stream_ptr)))
@@ -282,6 +290,52 @@ class Handle:
         out = CM()
         self._check(lib().spgemm_multiply(self._h, A, B, C.byref(out)))
         return out
+
+    # -- batched products (device operands) --------------------------------
+    def batch_plan(self, A_list, B_list) -> int:
+        """Plan and run the batch C_i = A_i * B_i once; returns total nnz."""
+        n = len(A_list)
+        if len(B_list) != n:
+            raise ValueError("A_list and B_list differ in length")
+        self._batch_A = (CM * n)(*A_list)
+        self._batch_B = (CM * n)(*B_list)
+        self._batch_count = n
+        tot = C.c_longlong(0)
+        self._check(lib().spgemm_batch_plan(self._h, n, self._batch_A, self._batch_B,
+                                            C.byref(tot)))
+        return tot.value
+
+    def batch_execute(self, graph: bool = True) -> None:
+        self._check(lib().spgemm_batch_execute(self._h, 1 if graph else 0))
+
+    def batch_offsets(self):
+        n = self._batch_count
+        ro = np.zeros(n + 1, np.int64)
+        no = np.zeros(n + 1, np.int64)
+        self._check(lib().spgemm_batch_offsets(
+            self._h, ro.ctypes.data_as(C.POINTER(C.c_longlong)),
+            no.ctypes.data_as(C.POINTER(C.c_longlong))))
+        return ro, no
+
+    def batch_result(self, i: int) -> CM:
+        out = CM()
+        self._check(lib().spgemm_batch_result(self._h, i, C.byref(out)))
+        return out
+
+    def batch_copy_all(self, rowptr_ptr: int, col_ptr: int, val_ptr: int) -> None:
+        """Copy the packed batch output to host memory at the given addresses."""
+        self._check(lib().spgemm_batch_copy_all(self._h, C.c_void_p(rowptr_ptr),
+                                                C.c_void_p(col_ptr), C.c_void_p(val_ptr)))
+
+    def batch_copy_result(self, i: int) -> Csr:
+        d = self.batch_result(i)
+        rowptr = np.zeros(d.num_rows + 1, np.int32)
+        col = np.zeros(max(d.nnz, 1), np.int32)
+        val = np.zeros(max(d.nnz, 1), np.float32)
+        self._check(lib().spgemm_batch_copy_result(
+            self._h, i, rowptr.ctypes.data_as(C.POINTER(C.c_int)),
+            col.ctypes.data_as(C.POINTER(C.c_int)), val.ctypes.data_as(C.POINTER(C.c_float))))
+        return Csr(d.num_rows, d.num_cols, rowptr, col[:d.nnz], val[:d.nnz])
 
 
 def multiply(A, B: Csr, precision: int = PLAIN) -> Csr:

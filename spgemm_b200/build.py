@@ -24,6 +24,7 @@ LIB = PKG / "libspgemm_b200.so"
 
 SOURCES = [
     "engine.cu",
+    "batch.cu",
     "api.cu",
     "legacy_mm.cu",
     "host_coo.cpp",

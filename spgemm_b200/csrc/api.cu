@@ -7,11 +7,7 @@
 #include <new>
 
 #include "../../include/spgemm_b200.h"
-#include "engine.h"
-
-struct spgemm_context {
-  sg::Engine eng;
-};
+#include "context.h"
 
 namespace {
 
@@ -143,6 +139,38 @@ int spgemm_numeric(spgemm_handle_t h, int* c_rowptr, int* c_colidx, float* c_val
 int spgemm_multiply(spgemm_handle_t h, cm A, cm B, cm* C) {
   if (!h) return SPGEMM_ERR_INVALID;
   return h->eng.multiply(A, B, C);
+}
+
+int spgemm_batch_plan(spgemm_handle_t h, int count, const cm* A, const cm* B,
+                      long long* nnz_total) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.plan(h->eng, count, A, B, nnz_total);
+}
+
+int spgemm_batch_execute(spgemm_handle_t h, int use_graph) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.execute(h->eng, use_graph);
+}
+
+int spgemm_batch_offsets(spgemm_handle_t h, long long* row_offsets, long long* nnz_offsets) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.offsets(h->eng, row_offsets, nnz_offsets);
+}
+
+int spgemm_batch_result(spgemm_handle_t h, int i, cm* C) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.result(h->eng, i, C);
+}
+
+int spgemm_batch_copy_result(spgemm_handle_t h, int i, int* c_rowptr, int* c_colidx,
+                             float* c_val) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.copy_result(h->eng, i, c_rowptr, c_colidx, c_val);
+}
+
+int spgemm_batch_copy_all(spgemm_handle_t h, int* c_rowptr, int* c_colidx, float* c_val) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  return h->batch.copy_all(h->eng, c_rowptr, c_colidx, c_val);
 }
 
 int spgemm_get_stats(spgemm_handle_t h, spgemm_stats* out) {

@@ -235,6 +235,7 @@ int Engine::symbolic(const cm& A, const cm& B, long long* nnz_c) {
 int Engine::analyze(const cm& A, const cm& B) {
   have_sym_ = false;
   have_analysis_ = false;
+  if (!replay_) ++epoch_;
   if (B.type != ROW_MAJOR) return fail(1, "B must be CSR (type ROW_MAJOR)");
   if (A.num_rows < 0 || A.num_cols < 0 || B.num_cols < 0 || A.nnz < 0 || B.nnz < 0)
     return fail(1, "negative dimension or nnz");
@@ -329,6 +330,10 @@ int Engine::analyze(const cm& A, const cm& B) {
   }
   // temporary-buffer slots of the fused rows (grand total = buffer size)
   if (int r = scan_counts(tcap_.as<int>(), m, toff_.as<long long>())) return r;
+  if (replay_) {  // same structure as the planned run: keep its sizes
+    have_analysis_ = true;
+    return 0;
+  }
   SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
         "read counters");
   SG_CK(cudaStreamSynchronize(stream_), "sync after row analysis");
@@ -386,6 +391,10 @@ int Engine::symbolic_pass(long long* nnz_c) {
         &dc->status, tr);
     SG_LAUNCHED("k_num_bin");
   }
+  if (replay_) {
+    have_sym_ = true;
+    return 0;
+  }
   SG_CK(cudaMemcpyAsync(host_counters_, dc, sizeof(DevCounters), cudaMemcpyDeviceToHost, stream_),
         "read counters");
   SG_CK(cudaStreamSynchronize(stream_), "sync after symbolic pass");
@@ -395,7 +404,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
   nslices_ = host_counters_->slice_count;
   nmid_ = host_counters_->mid_count;
   overflow_rows_ = host_counters_->overflow_count;
-  if (nnz_c_ > 2147483647ll)
+  if (nnz_c_ > 2147483647ll && !batch_out_)
     return fail(4, "nnz(C) = " + std::to_string(nnz_c_) + " exceeds the int32 range of cm");
   if (nnz_c) *nnz_c = nnz_c_;
   have_sym_ = true;
@@ -410,7 +419,7 @@ int Engine::launch_first_pass() {
   int* c_cnt = c_cnt_.as<int>();
   const long long* row_p = row_p_.as<long long>();
   int* rows = sym_rows_.as<int>();
-  bitmap_words_ = 0;
+  if (!replay_) bitmap_words_ = 0;
   // long rows first: they are the heaviest work items
   if (fb_counts_[FB_LONG] > 0) {
     const int win = std::min(n_, tn_.sym_window);
@@ -425,7 +434,7 @@ int Engine::launch_first_pass() {
       SG_CK(restrict_scratch_.ensure(16), "alloc restrict scratch");
     // Keep the long rows' presence bitmaps for the numeric pass when they fit
     // in a modest share of free device memory; otherwise it rebuilds them.
-    if (tn_.keep_bitmaps) {
+    if (tn_.keep_bitmaps && !replay_) {
       const size_t words = (size_t)(n_ + 31) / 32;
       const size_t want = words * 4 * (size_t)cnt;
       size_t free_b = 0, total_b = 0;
@@ -520,9 +529,9 @@ int Engine::launch_fused() {
 template int Engine::launch_fused<0>();
 template int Engine::launch_fused<1>();
 
-int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
+int Engine::numeric_values(int* c_col, float* c_val) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
-  if (!c_rowptr || (nnz_c_ > 0 && (!c_col || !c_val))) return fail(1, "null output pointer");
+  if (nnz_c_ > 0 && (!c_col || !c_val)) return fail(1, "null output pointer");
   if (m_ > 0 && temp_total_ > 0) {
     prof_begin("k_copy_fused");
     k_copy_fused<<<blocks_for((long long)m_ * 32, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
@@ -530,11 +539,11 @@ int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
         t_col_.as<int>(), t_val_.as<float>(), c_col, c_val);
     SG_LAUNCHED("k_copy_fused");
   }
-  if (int r = launch_numeric_bins(c_col, c_val)) return r;
-  prof_begin("k_rowptr_to_i32");
-  k_rowptr_to_i32<<<blocks_for(m_ + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
-      c_rowptr64_.as<long long>(), m_ + 1, c_rowptr);
-  SG_LAUNCHED("k_rowptr_to_i32");
+  return launch_numeric_bins(c_col, c_val);
+}
+
+int Engine::finish_numeric() {
+  if (replay_) return 0;  // the caller reads the status after the captured work
   DevCounters* dc = counters_.as<DevCounters>();
   SG_CK(cudaMemcpyAsync(&host_counters_->status, &dc->status, sizeof(unsigned),
                         cudaMemcpyDeviceToHost, stream_),
@@ -542,6 +551,40 @@ int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
   SG_CK(cudaStreamSynchronize(stream_), "sync after numeric pass");
   prof_collect();
   return check_status(host_counters_->status);
+}
+
+int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
+  if (!c_rowptr) return fail(1, "null output pointer");
+  if (int r = numeric_values(c_col, c_val)) return r;
+  prof_begin("k_rowptr_to_i32");
+  k_rowptr_to_i32<<<blocks_for(m_ + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+      c_rowptr64_.as<long long>(), m_ + 1, c_rowptr);
+  SG_LAUNCHED("k_rowptr_to_i32");
+  return finish_numeric();
+}
+
+int Engine::numeric_batch(int count, const long long* row_off_dev, long long max_rows,
+                          int* c_rowptr, int* c_col, float* c_val) {
+  if (!c_rowptr) return fail(1, "null output pointer");
+  if (int r = numeric_values(c_col, c_val)) return r;
+  if (count > 0) {
+    prof_begin("k_batch_rowptr");
+    const dim3 grid(blocks_for(max_rows + 1, 256, 64), count);
+    k_batch_rowptr<<<grid, 256, 0, stream_>>>(c_rowptr64_.as<long long>(), row_off_dev, c_rowptr);
+    SG_LAUNCHED("k_batch_rowptr");
+  }
+  return finish_numeric();
+}
+
+int Engine::read_status(unsigned* st) {
+  DevCounters* dc = counters_.as<DevCounters>();
+  SG_CK(cudaMemcpyAsync(&host_counters_->status, &dc->status, sizeof(unsigned),
+                        cudaMemcpyDeviceToHost, stream_),
+        "read status");
+  SG_CK(cudaStreamSynchronize(stream_), "sync after batch");
+  prof_collect();
+  *st = host_counters_->status;
+  return check_status(*st);
 }
 
 int Engine::launch_numeric_bins(int* c_col, float* c_val) {

@@ -59,10 +59,32 @@ class Engine {
   // Phase 2 into caller-provided device buffers; synchronises once to
   // check the status word.
   int numeric(int* c_rowptr, int* c_col, float* c_val);
+  // Phase 2 for a block-diagonal batch: C's row pointers are written per
+  // product (product i's m_i + 1 entries, from 0, at c_rowptr + row_off[i] + i;
+  // row_off_dev holds count + 1 row offsets on the device), columns and values
+  // at their global positions. Allows nnz(C) beyond the int32 range.
+  int numeric_batch(int count, const long long* row_off_dev, long long max_rows, int* c_rowptr,
+                    int* c_col, float* c_val);
   // Both phases into engine-owned output buffers.
   int multiply(const cm& A, const cm& B, cm* C_dev);
   // Numeric pass of the current symbolic result into engine-owned buffers.
   int multiply_numeric_owned(cm* C_dev);
+
+  // Replay mode: the operands have the structure of the last product run
+  // with replay off, so the host keeps that run's sizes, bin counts and
+  // grids and the pipeline makes no host synchronisation (it can then be
+  // recorded by stream capture). The status word is read by read_status().
+  void set_replay(bool on) { replay_ = on; }
+  bool replay() const { return replay_; }
+  // Batch output: nnz(C) may exceed the int32 range of a single cm.
+  void set_batch_output(bool on) { batch_out_ = on; }
+  int read_status(unsigned* st);
+  const long long* rowptr64() const { return c_rowptr64_.as<long long>(); }
+  void add_launches(long long n) { launches_ += n; }
+  // Incremented by every analysis run outside replay mode: device buffers
+  // and host sizes of an earlier product may have changed since.
+  long long epoch() const { return epoch_; }
+  bool profiling() const { return prof_on_; }
 
   const std::string& last_error() const { return err_; }
   long long launches() const { return launches_; }
@@ -97,6 +119,8 @@ class Engine {
   int cuda_fail(cudaError_t e, const char* what);
 
  private:
+  int numeric_values(int* c_col, float* c_val);
+  int finish_numeric();
   int launch_first_pass();
   template <int MODE> int launch_fused();
   int launch_numeric_bins(int* c_col, float* c_val);
@@ -114,6 +138,10 @@ class Engine {
   std::string err_;
   long long launches_ = 0;
   std::unordered_map<const void*, size_t> smem_set_;
+
+  bool replay_ = false;
+  bool batch_out_ = false;
+  long long epoch_ = 0;
 
   // current product
   bool have_sym_ = false;

@@ -490,6 +490,20 @@ __global__ void k_rowptr_to_i32(const long long* __restrict__ in, int n1,
 }
 
 // int32 CSC/CSR pointer array from counts (used by the transpose).
+// Row pointers of a block-diagonal batch, per product: product p =
+// blockIdx.y owns the global rows [row_off[p], row_off[p + 1]); its m_p + 1
+// pointers, relative to its first entry, go to out[row_off[p] + p ...].
+__global__ void __launch_bounds__(256)
+k_batch_rowptr(const long long* __restrict__ rowptr64, const long long* __restrict__ row_off,
+               int* __restrict__ out) {
+  const int p = blockIdx.y;
+  const long long r0 = row_off[p], r1 = row_off[p + 1];
+  const long long base = rowptr64[r0];
+  for (long long r = r0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; r <= r1;
+       r += (long long)gridDim.x * blockDim.x)
+    out[r + p] = (int)(rowptr64[r] - base);
+}
+
 __global__ void k_rowptr_i64_to_i32_shift(const long long* __restrict__ in, int n1,
                                           int* __restrict__ out, int* __restrict__ out2) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n1; i += gridDim.x * blockDim.x) {

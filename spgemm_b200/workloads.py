@@ -69,15 +69,22 @@ def from_coo(rows: int, cols: int, r: np.ndarray, c: np.ndarray, v: np.ndarray) 
     """CSR from coordinate arrays (duplicates must already be removed)."""
     r = np.asarray(r, np.int64)
     c = np.asarray(c, np.int64)
-    order = np.lexsort((c, r))
-    r, c, v = r[order], c[order], np.asarray(v, np.float32)[order]
+    v = np.asarray(v, np.float32)
+    key = r * cols + c
+    if len(key) > 1 and not bool(np.all(key[1:] >= key[:-1])):
+        order = np.lexsort((c, r))
+        r, c, v = r[order], c[order], v[order]
     rowptr = np.zeros(rows + 1, np.int64)
-    np.add.at(rowptr, r + 1, 1)
-    return Csr(rows, cols, np.cumsum(rowptr).astype(np.int32), c.astype(np.int32), v)
+    rowptr[1:] = np.cumsum(np.bincount(r, minlength=rows)[:rows])
+    return Csr(rows, cols, rowptr.astype(np.int32), c.astype(np.int32), v)
 
 
 def _unique_keys(keys: np.ndarray) -> np.ndarray:
-    return np.unique(keys)
+    """Sorted distinct values (np.unique's result, by sorting)."""
+    keys = np.sort(keys)
+    if len(keys) < 2:
+        return keys
+    return keys[np.concatenate(([True], keys[1:] != keys[:-1]))]
 
 
 def _rows_without_replacement(rng, n_rows: int, n_cols: int, deg: np.ndarray) -> tuple:
@@ -152,7 +159,7 @@ def rmat(scale: int, edge_factor: float, seed: int, a=0.57, b=0.19, c=0.19,
         got += len(r)
     r = np.concatenate(rs)
     cc = np.concatenate(cs)
-    keys = np.unique(r * n + cc)
+    keys = _unique_keys(r * n + cc)
     r, cc = keys // n, keys % n
     if values == "unit_open":
         v = (1.0 - rng.random(len(r))).astype(np.float32)
@@ -221,14 +228,55 @@ def batch_specs(count: int, seed: int, n_lo=1000, n_hi=200000, lam_lo=4.0, lam_h
             for i in range(count)]
 
 
+def _rmat_columns(rng, size: int, n: int, col_bit_p: float) -> np.ndarray:
+    """`size` columns in [0, n) from the R-MAT column marginal: each of the
+    ceil(log2 n) bits is 1 with probability col_bit_p (b + d of the R-MAT
+    quadrant probabilities), values >= n redrawn."""
+    scale = max(int(np.ceil(np.log2(max(n, 2)))), 1)
+    out = np.empty(size, np.int64)
+    todo = np.arange(size)
+    while len(todo):
+        c = np.zeros(len(todo), np.int64)
+        for bit in range(scale - 1, -1, -1):
+            c |= (rng.random(len(todo)) < col_bit_p).astype(np.int64) << bit
+        ok = c < n
+        out[todo[ok]] = c[ok]
+        todo = todo[~ok]
+    return out
+
+
+def rmat_poisson(n: int, lam: float, seed: int, b=0.19, d=0.05, low=-1.0, high=1.0) -> Csr:
+    """Row lengths Poisson(lam) (at most n), columns distinct within a row and
+    drawn from the R-MAT column marginal (bit probability b + d): the R-MAT
+    pattern's skewed column popularity with bounded rows."""
+    rng = np.random.default_rng(seed)
+    deg = np.minimum(rng.poisson(lam, size=n).astype(np.int64), n)
+    keys = np.empty(0, np.int64)
+    need = deg.copy()
+    for _ in range(64):
+        tot = int(need.sum())
+        if tot == 0:
+            break
+        r = np.repeat(np.arange(n, dtype=np.int64), need)
+        c = _rmat_columns(rng, tot, n, b + d)
+        keys = _unique_keys(np.concatenate([keys, r * n + c]))
+        have = np.bincount(keys // n, minlength=n)
+        need = np.maximum(deg - have, 0)
+    r, c = keys // n, keys % n
+    v = rng.uniform(low, high, size=len(r)).astype(np.float32)
+    return from_coo(n, n, r, c, v)
+
+
 def batch_item(kind: str, n: int, lam: float, seed: int) -> BatchItem:
+    """One product of the batch: A and B n x n, Poisson(lam) entries per row,
+    columns uniform ("er") or from the R-MAT column marginal ("rmat"),
+    values U[-1, 1]; independent patterns for A and B."""
     if kind == "er":
         A = er_poisson(n, lam, seed * 2 + 0)
         B = er_poisson(n, lam, seed * 2 + 1)
     else:
-        scale = max(int(np.ceil(np.log2(n))), 1)
-        A = rmat(scale, lam, seed * 2 + 0, n=n, values="sym")
-        B = rmat(scale, lam, seed * 2 + 1, n=n, values="sym")
+        A = rmat_poisson(n, lam, seed * 2 + 0)
+        B = rmat_poisson(n, lam, seed * 2 + 1)
     return BatchItem(kind, n, lam, seed, A, B)
 
 
