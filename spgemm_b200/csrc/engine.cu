@@ -476,7 +476,7 @@ int Engine::launch_fused() {
     const int b = L - 6, cnt = fb_counts_[b];                                                  \
     if (cnt > 0) {                                                                             \
       overflow_bound += cnt;                                                                   \
-      const size_t smem = WPB * ((size_t(1) << L) * (VB + 4) + SEG_SCRATCH_BYTES);             \
+      const size_t smem = WPB * ((size_t(1) << L) * (VB + 5) + SEG_SCRATCH_BYTES);             \
       SG_CK(smem_attr(k_fused_warp<L, MODE>, smem), "smem attr k_fused_warp");                 \
       prof_begin("k_fused_warp<" #L ">");                                                      \
       k_fused_warp<L, MODE><<<blocks_for(cnt, WPB, (long long)sms_ * 16), SW_THREADS, smem,    \
@@ -554,6 +554,7 @@ int Engine::finish_numeric() {
 }
 
 int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
+  if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
   if (!c_rowptr) return fail(1, "null output pointer");
   if (int r = numeric_values(c_col, c_val)) return r;
   prof_begin("k_rowptr_to_i32");
@@ -565,6 +566,7 @@ int Engine::numeric(int* c_rowptr, int* c_col, float* c_val) {
 
 int Engine::numeric_batch(int count, const long long* row_off_dev, long long max_rows,
                           int* c_rowptr, int* c_col, float* c_val) {
+  if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
   if (!c_rowptr) return fail(1, "null output pointer");
   if (int r = numeric_values(c_col, c_val)) return r;
   if (count > 0) {

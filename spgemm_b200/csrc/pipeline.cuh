@@ -185,12 +185,22 @@ template <int MODE> struct SlotOf { using T = float; };
 template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or double bits
 
 // Fused pass, one warp per row: hash accumulate, compact the table in place,
-// bitonic-sort the occupied entries, write the sorted row to the temporary
+// sort the occupied entries by column, write the sorted row to the temporary
 // buffer at toff[i] and its length to c_cnt[i]. A row that turns out to have
 // more distinct columns than 4/5 of the table is pushed to the mid list (span
 // within mid_cols) or the largest block list and redone there.
+//
+// Sorting: tables of 256 slots and more sort packed keys (column offset in
+// the row's span above the slot index; the values stay in their slots) by a
+// bucket pass -- NB = T/4 buckets on the column offset's top bits, counts,
+// scan, scatter with the keys held in registers -- and an insertion sort of
+// each bucket by one lane. Rows whose columns crowd one bucket (more than
+// BUCKET_MAX entries) or whose span is too wide to pack sort the packed keys
+// (or key/value pairs) bitonically instead.
+constexpr int BUCKET_MAX = 24;
+
 template <int LOG2T, int MODE>
-__global__ void __launch_bounds__(SW_THREADS, 4)
+__global__ void __launch_bounds__(SW_THREADS, LOG2T >= 10 ? 2 : 4)
 k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
              const int2* __restrict__ row_span, const long long* __restrict__ toff,
              int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
@@ -206,6 +216,10 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
   V* vals = reinterpret_cast<V*>(smem) + warp * T;
   unsigned* keys = reinterpret_cast<unsigned*>(smem + WPB * T * sizeof(V)) + warp * T;
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem + WPB * T * (sizeof(V) + 4)) + warp;
+  constexpr int NB = T / 4;                   // sort buckets (tables of >= 256 slots)
+  constexpr int E = (LIMIT + 31) / 32;        // entries per lane
+  int* bucket = reinterpret_cast<int*>(smem + WPB * (T * (sizeof(V) + 4) + sizeof(SegScratch))) +
+                warp * NB;
   for (int r = blockIdx.x * WPB + warp; r < nrows; r += gridDim.x * WPB) {
     const int i = rows[r];
     for (int t = lane; t < T; t += 32) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
@@ -241,14 +255,88 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
     }
     int n2 = 1;
     while (n2 < o) n2 <<= 1;
-    for (int t = o + lane; t < n2; t += 32) keys[t] = EMPTY_KEY;
-    __syncwarp();
-    bitonic_sort_kv_rt(keys, vals, n2, lane, 32, WarpSync());
     const long long base = toff[i];
-    for (int t = lane; t < o; t += 32) {
-      t_col[base + t] = (int)keys[t];
-      if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
-      else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    const int2 sp = row_span[i];
+    const unsigned lo = (unsigned)(sp.x & ~31);
+    const unsigned span = (unsigned)(sp.y + 1) - lo;
+    if (LOG2T >= 8 && o > 64 && span <= (1u << (32 - LOG2T))) {
+      // packed keys: (column - lo) << LOG2T | slot
+      unsigned pk[E];
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int t = lane + 32 * e;
+        pk[e] = t < o ? ((keys[t] - lo) << LOG2T) | (unsigned)t : EMPTY_KEY;
+      }
+      const int bits = 32 - __clz(span > 1 ? span - 1 : 1);
+      const int shift = bits > LOG2T - 2 ? bits - (LOG2T - 2) : 0;
+      for (int t = lane; t < NB; t += 32) bucket[t] = 0;
+      __syncwarp();
+#pragma unroll
+      for (int e = 0; e < E; ++e)
+        if (pk[e] != EMPTY_KEY) atomicAdd(&bucket[(pk[e] >> LOG2T) >> shift], 1);
+      __syncwarp();
+      constexpr int PER = NB / 32 > 0 ? NB / 32 : 1;
+      int cnt[PER];
+      int sum = 0, mx = 0;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        cnt[q] = bucket[lane * PER + q];
+        sum += cnt[q];
+        mx = max(mx, cnt[q]);
+      }
+#pragma unroll
+      for (int d = 16; d > 0; d >>= 1) mx = max(mx, __shfl_xor_sync(FULL, mx, d));
+      if (mx <= BUCKET_MAX) {
+        int run = warp_incl_scan(sum) - sum;
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+          bucket[lane * PER + q] = run;
+          run += cnt[q];
+        }
+        __syncwarp();
+        // every key is in registers: scatter into the key array by bucket
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (pk[e] != EMPTY_KEY) keys[atomicAdd(&bucket[(pk[e] >> LOG2T) >> shift], 1)] = pk[e];
+        __syncwarp();
+        // bucket b now ends at bucket[b]; each lane sorts its buckets in place
+        for (int b = lane; b < NB; b += 32) {
+          const int s0 = b ? bucket[b - 1] : 0, s1 = bucket[b];
+          for (int x = s0 + 1; x < s1; ++x) {
+            const unsigned v = keys[x];
+            int y = x - 1;
+            while (y >= s0 && keys[y] > v) {
+              keys[y + 1] = keys[y];
+              --y;
+            }
+            keys[y + 1] = v;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < E; ++e)
+          if (lane + 32 * e < n2) keys[lane + 32 * e] = pk[e];
+        for (int t = E * 32 + lane; t < n2; t += 32) keys[t] = EMPTY_KEY;
+        __syncwarp();
+        bitonic_sort_keys_rt(keys, n2, lane, 32, WarpSync());
+      }
+      __syncwarp();
+      for (int t = lane; t < o; t += 32) {
+        const unsigned p = keys[t];
+        const int slot = (int)(p & (T - 1));
+        t_col[base + t] = (int)(lo + (p >> LOG2T));
+        if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[slot]);
+        else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[slot]);
+      }
+    } else {
+      for (int t = o + lane; t < n2; t += 32) keys[t] = EMPTY_KEY;
+      __syncwarp();
+      bitonic_sort_kv_rt(keys, vals, n2, lane, 32, WarpSync());
+      for (int t = lane; t < o; t += 32) {
+        t_col[base + t] = (int)keys[t];
+        if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+        else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+      }
     }
     if (lane == 0) c_cnt[i] = o;
     __syncwarp();
