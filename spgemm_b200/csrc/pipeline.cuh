@@ -195,8 +195,9 @@ template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or do
 // bucket pass -- NB = T/4 buckets on the column offset's top bits, counts,
 // scan, scatter with the keys held in registers -- and an insertion sort of
 // each bucket by one lane. Rows whose columns crowd one bucket (more than
-// BUCKET_MAX entries) or whose span is too wide to pack sort the packed keys
-// (or key/value pairs) bitonically instead.
+// BUCKET_MAX entries: skewed column popularity) take LSD radix passes over
+// the column offset instead; rows whose span is too wide to pack, and small
+// tables, sort key/value pairs bitonically.
 constexpr int BUCKET_MAX = 24;
 
 template <int LOG2T, int MODE>
@@ -313,12 +314,53 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
           }
         }
       } else {
+        // crowded buckets (skewed columns): LSD radix sort of the column
+        // offset, LOG2T - 2 bits (NB counters) a pass, stable by array order;
+        // each pass scatters from registers into the key array, then reloads
+        // the keys in the new order
+        constexpr int DIG = LOG2T - 2;
+        for (int d0 = 0; d0 < bits; d0 += DIG) {
+          for (int t = lane; t < NB; t += 32) bucket[t] = 0;
+          __syncwarp();
 #pragma unroll
-        for (int e = 0; e < E; ++e)
-          if (lane + 32 * e < n2) keys[lane + 32 * e] = pk[e];
-        for (int t = E * 32 + lane; t < n2; t += 32) keys[t] = EMPTY_KEY;
-        __syncwarp();
-        bitonic_sort_keys_rt(keys, n2, lane, 32, WarpSync());
+          for (int e = 0; e < E; ++e)
+            if (pk[e] != EMPTY_KEY) atomicAdd(&bucket[((pk[e] >> LOG2T) >> d0) & (NB - 1)], 1);
+          __syncwarp();
+          int tot = 0;
+#pragma unroll
+          for (int q = 0; q < PER; ++q) {
+            cnt[q] = bucket[lane * PER + q];
+            tot += cnt[q];
+          }
+          int run = warp_incl_scan(tot) - tot;
+#pragma unroll
+          for (int q = 0; q < PER; ++q) {
+            bucket[lane * PER + q] = run;
+            run += cnt[q];
+          }
+          __syncwarp();
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const bool valid = pk[e] != EMPTY_KEY;
+            const unsigned dig = valid ? ((pk[e] >> LOG2T) >> d0) & (NB - 1) : (unsigned)(NB + lane);
+            const unsigned peers = __match_any_sync(FULL, dig);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            int pos = 0;
+            if (valid) pos = bucket[dig] + rank;
+            __syncwarp();
+            if (valid) {
+              keys[pos] = pk[e];
+              if (rank == __popc(peers) - 1) bucket[dig] = pos + 1;
+            }
+            __syncwarp();
+          }
+#pragma unroll
+          for (int e = 0; e < E; ++e) {
+            const int t = lane + 32 * e;
+            pk[e] = t < o ? keys[t] : EMPTY_KEY;
+          }
+          __syncwarp();
+        }
       }
       __syncwarp();
       for (int t = lane; t < o; t += 32) {

@@ -161,3 +161,19 @@ def test_batch_rejects_mixed_formats_and_bad_shapes():
         with pytest.raises(sg.SpgemmError) as e:
             h.batch_execute()
         assert e.value.status == 5  # no successful plan
+
+
+@pytest.mark.parametrize("precision", [sg.PLAIN, sg.COMPENSATED])
+def test_batch_large_warp_tables(precision):
+    # 1024-slot warp tables: uniform (ER) rows take the bucket sort, rows with
+    # R-MAT-skewed columns crowd the low buckets and take the radix passes
+    pairs = small_batch(12, 31, n_lo=3000, n_hi=30000)
+    db = DeviceBatch(pairs)
+    with sg.Handle(precision) as h:
+        h.set_tuning(warp_table_max=1024, warp_p_max=1024, warp_cap_max=2048)
+        h.batch_plan(db.A, db.B)
+        st = h.stats()
+        assert st["rows_per_symbolic_bin"][4] > 0  # rows in 1024-slot tables
+        refs = check_all(h, pairs, precision)
+        h.batch_execute(graph=True)
+        check_all(h, pairs, precision, refs)
