@@ -676,6 +676,28 @@ __device__ __forceinline__ void bitonic_sort_kv_rt(unsigned* keys, V* vals, int 
   }
 }
 
+// bitonic_sort_kv_rt for keys alone (n a power of two, keys unique or padded
+// with EMPTY_KEY), by the threads of one warp or block.
+template <class Sync>
+__device__ __forceinline__ void bitonic_sort_keys_rt(unsigned* keys, int n, int tid, int nthreads,
+                                                     Sync sync) {
+  for (int k = 2; k <= n; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = tid; t < (n >> 1); t += nthreads) {
+        const int lo = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+        const int hi = lo + j;
+        const bool up = (lo & k) == 0;
+        const unsigned kl = keys[lo], kh = keys[hi];
+        if ((kl > kh) == up) {
+          keys[lo] = kh;
+          keys[hi] = kl;
+        }
+      }
+      sync();
+    }
+  }
+}
+
 struct LongValTwoSum {
   const uint2* dir;
   float2* vals;

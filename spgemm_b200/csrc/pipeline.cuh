@@ -196,9 +196,11 @@ template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or do
 // scan, scatter with the keys held in registers -- and an insertion sort of
 // each bucket by one lane. Rows whose columns crowd one bucket (more than
 // BUCKET_MAX entries: skewed column popularity) take LSD radix passes over
-// the column offset instead; rows whose span is too wide to pack, and small
-// tables, sort key/value pairs bitonically.
+// the column offset instead. Rows of at most SMALL_SORT entries (and small
+// tables) sort the packed keys bitonically; rows whose span is too wide to
+// pack sort key/value pairs bitonically.
 constexpr int BUCKET_MAX = 24;
+constexpr int SMALL_SORT = 128;  // rows with at most this many entries sort bitonically
 
 template <int LOG2T, int MODE>
 __global__ void __launch_bounds__(SW_THREADS, LOG2T >= 10 ? 2 : 4)
@@ -260,7 +262,20 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
     const int2 sp = row_span[i];
     const unsigned lo = (unsigned)(sp.x & ~31);
     const unsigned span = (unsigned)(sp.y + 1) - lo;
-    if (LOG2T >= 8 && o > 64 && span <= (1u << (32 - LOG2T))) {
+    if (span <= (1u << (32 - LOG2T)) && (LOG2T < 8 || o <= SMALL_SORT)) {
+      // packed keys, (column - lo) << LOG2T | slot, sorted bitonically
+      for (int t = lane; t < n2; t += 32)
+        keys[t] = t < o ? ((keys[t] - lo) << LOG2T) | (unsigned)t : EMPTY_KEY;
+      __syncwarp();
+      bitonic_sort_keys_rt(keys, n2, lane, 32, WarpSync());
+      for (int t = lane; t < o; t += 32) {
+        const unsigned p = keys[t];
+        const int slot = (int)(p & (T - 1));
+        t_col[base + t] = (int)(lo + (p >> LOG2T));
+        if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[slot]);
+        else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[slot]);
+      }
+    } else if (LOG2T >= 8 && span <= (1u << (32 - LOG2T))) {
       // packed keys: (column - lo) << LOG2T | slot
       unsigned pk[E];
 #pragma unroll
