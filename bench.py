@@ -225,6 +225,21 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ncu summaries (profiles/) of the dominant kernel's DRAM traffic per launch,
+# by (workload, kernel): the roofline's "traffic" field.
+TRAFFIC_PROFILES = {("rmat18", "k_num_long"): ROOT / "profiles" / "k_num_long_rmat18_traffic.md"}
+
+
+def profiled_traffic(workload, kernel):
+    p = TRAFFIC_PROFILES.get((workload, kernel))
+    if p is None or not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return int(line.split(":", 1)[1].strip())
+    return None
+
+
 def measured_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -675,9 +690,11 @@ def main():
                 alg = algorithmic_bytes(sel, p_i, a_len, o_i, b_touched, products, with_c=writes_c)
                 per_launch = alg * args.steps / cnt
                 avg_s = ms / cnt / 1e3
+                wl_key = f"rmat{args.scale}" if args.workload == "rmat" else args.workload
                 roof = {"bound": "hbm", "kernel": name, "achieved": per_launch / avg_s / 1e9,
                         "peak": peak, "unit": "GB/s", "frac": per_launch / avg_s / 1e9 / peak,
-                        "traffic": None, "algorithmic_bytes_per_launch": per_launch,
+                        "traffic": profiled_traffic(wl_key, name),
+                        "algorithmic_bytes_per_launch": per_launch,
                         "avg_launch_ms": ms / cnt, "peak_kind": peak_kind}
 
     # e2e through the host-buffer C ABI (pinned host memory)
