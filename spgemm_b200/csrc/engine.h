@@ -80,6 +80,11 @@ class Engine {
   void set_batch_output(bool on) { batch_out_ = on; }
   int read_status(unsigned* st);
   const long long* rowptr64() const { return c_rowptr64_.as<long long>(); }
+  // After analyze(): products per row (int64) and the row list of first-pass
+  // bin b (sym_bin_rows(b) entries).
+  const long long* row_products() const { return row_p_.as<long long>(); }
+  const int* bin_list(int b) const { return sym_rows_.as<int>() + (size_t)b * (size_t)m_; }
+  const int* a_rowptr() const { return op_.a_rowptr; }
   void add_launches(long long n) { launches_ += n; }
   // Incremented by every analysis run outside replay mode: device buffers
   // and host sizes of an earlier product may have changed since.

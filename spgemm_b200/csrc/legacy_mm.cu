@@ -95,6 +95,9 @@ extern "C" {
 
 void spgemm_set_exit_on_error(int enable) { g_exit_on_error = enable ? 1 : 0; }
 int spgemm_legacy_status(void) { return g_status; }
+// shared with the spGEMM.h family (legacy_spgemm.cu)
+int spgemm_internal_exit_on_error(void) { return g_exit_on_error; }
+void spgemm_internal_set_legacy_status(int s) { g_status = s; }
 
 // Replaces reference src/mm.cu:65-136 (kernel coo2cm at :43-63).
 cm cudaCOO2CM(coo mat) {
@@ -265,11 +268,43 @@ void cudaMergeGEMM(cm C) {
   }
 }
 
-// Declared in the reference (lib/mm.h:23) without a definition: symbolic
-// and numeric pass in one call.
+// Declared in the reference (lib/mm.h:23) without a definition, next to its
+// DenseChunk type (lib/mm.h:10-15: a column index and 64 dense values): the
+// dense-chunk strategy. Here: the whole product (symbolic and numeric pass)
+// with rows accumulated in dense column windows wherever their column span
+// allows -- the span-bitmap accumulator (a dense presence bitmap plus values
+// in column order) for every fused row with span <= 2^18 instead of warp hash
+// tables, and for long rows with few outputs instead of block hash tables.
+// Rows wider than that keep the hash paths. The handle's own tuning is
+// restored afterwards; the rows are re-binned for the product, so it may
+// follow cudaInitGEMM directly or replace cudaBinGEMM + cudaMergeGEMM.
 void cudaDCGEMM(cm A, cm B, cm C) {
+  (void)A;
+  (void)B;
+  g_status = SPGEMM_OK;
+  if (!g_have_a || !g_have_b) {
+    LEGACY_FAIL(SPGEMM_ERR_STATE, "cudaDCGEMM: convert A (COL_MAJOR) and B (ROW_MAJOR) first");
+    return;
+  }
+  sg::Engine& E = eng();
+  const sg::Tuning saved = E.tuning();
+  sg::Tuning dc = saved;
+  dc.warp_p_max = 0;        // no warp hash rows
+  dc.mid_cols = 1 << 18;    // dense windows up to 2^18 columns
+  dc.mid_o_min = 0;         // long rows with few outputs: dense windows too
+  if (int r = E.set_tuning(dc)) {
+    LEGACY_FAIL(r, E.last_error().c_str());
+    return;
+  }
+  g_have_c = false;
+  if (int r = E.analyze(g_A_dev, g_B_dev)) {
+    E.set_tuning(saved);
+    LEGACY_FAIL(r, E.last_error().c_str());
+    return;
+  }
   cudaBinGEMM(A, B, C);
   if (g_status == SPGEMM_OK) cudaMergeGEMM(C);
+  E.set_tuning(saved);
 }
 
 int spgemm_get_result(cm* out) {
