@@ -22,8 +22,9 @@ extern "C" {
 #include "coo.h"
 #include "cm.h"
 
-/* A 64-column dense accumulator chunk (reference lib/mm.h:10-15), used by
- * cudaDCGEMM's merge strategy. */
+/* A 64-column dense accumulator chunk (reference lib/mm.h:10-15); the
+ * struct is kept for binary compatibility (cudaDCGEMM's dense windows are
+ * bitmaps over the row's column span, not arrays of these). */
 struct DenseChunk
 {
     int idx;
@@ -47,9 +48,12 @@ void cudaSimpleGEMM(cm A, cm B, cm C);
 /* Symbolic pass per bin (exact nnz of every C row, row pointers).
  * Replaces reference src/mm.cu:314-327. */
 void cudaBinGEMM(cm A, cm B, cm C);
-/* Symbolic + numeric pass using 64-column dense chunks as the merge
- * accumulator for every row. Declared but never defined in the reference
- * (lib/mm.h:23). */
+/* Symbolic + numeric pass with the dense-chunk strategy: every row whose
+ * column span is at most 2^18 accumulates in dense column windows (a
+ * presence bitmap plus values in column order) instead of hash tables; wider
+ * rows keep the hash paths. Re-bins the rows, so it may follow cudaInitGEMM
+ * directly. Prints "nnzC nnzCf" like cudaMergeGEMM. Declared but never
+ * defined in the reference (lib/mm.h:23). */
 void cudaDCGEMM(cm A, cm B, cm C);
 /* Numeric pass: merged, column-sorted C; prints "nnzC nnzCf" like the
  * reference. Replaces reference src/mm.cu:407-450. */

@@ -190,6 +190,22 @@ int spgemm_reset_kernel_times(spgemm_handle_t handle);
 int spgemm_get_kernel_times(spgemm_handle_t handle, char* names, int names_len,
                             double* ms, long long* launches, int max_kernels);
 
+/* Value-preserving Matrix-Market reader. The reference's readMTX
+ * (src/coo.cpp:110-173, kept unchanged in coo.h) forces every value to 1.1,
+ * reads the first size token as the column count and misparses pattern
+ * files; this reader follows the format: "coordinate" files with field real,
+ * double, integer or pattern (pattern entries get 1.0) and symmetry general,
+ * symmetric (mirrored off-diagonal entries), skew-symmetric (mirrored and
+ * negated) or hermitian (as symmetric; real fields only). Indices become
+ * 0-based; num_rows / num_cols come from the size line in the format's order
+ * (rows first); entries keep file order, mirrored ones right after their
+ * source entry; `type` is left as the caller set it (call sortCOO for the
+ * order cudaCOO2CM wants). out->data is malloc'd (freeCOO releases it).
+ * Returns SPGEMM_OK, SPGEMM_ERR_INVALID for an unreadable, malformed,
+ * truncated or out-of-range file (nothing is kept), SPGEMM_ERR_TOO_LARGE
+ * beyond INT32_MAX entries. No counterpart in the reference. */
+int spgemm_read_mtx(coo* out, const char* path);
+
 /* Allocation-free COO -> compressed conversion. This entry point has no
  * counterpart in the reference; it performs the conversion of cudaCOO2CM
  * (sorted triplets -> CSR for ROW_MAJOR, CSC for COL_MAJOR) on device arrays

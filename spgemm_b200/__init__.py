@@ -116,6 +116,7 @@ def lib():
         L.spgemm_batch_result.argtypes = [vp, C.c_int, C.POINTER(CM)]
         L.spgemm_batch_copy_result.argtypes = [vp, C.c_int, ip, ip, fp]
         L.spgemm_batch_copy_all.argtypes = [vp, vp, vp, vp]
+        L.spgemm_read_mtx.argtypes = [C.POINTER(COO), C.c_char_p]
         L.cmFree.argtypes = [C.POINTER(CM)]
         L.cudaCOO2CM.restype = CM
         L.cudaCOO2CM.argtypes = [COO]
@@ -133,6 +134,26 @@ def lib():
         L.initCOO.argtypes = [C.POINTER(COO)]
         _lib = L
     return _lib
+
+
+def read_mtx(path):
+    """Matrix-Market file through the library's value-preserving reader
+    (spgemm_read_mtx): (rows, cols, row indices, column indices, values) as
+    numpy arrays, entries in file order with mirrored ones after their source.
+    Raises SpgemmError on a malformed file."""
+    L = lib()
+    m = COO()
+    st = L.spgemm_read_mtx(C.byref(m), str(path).encode())
+    if st != 0:
+        raise SpgemmError(st, f"spgemm_read_mtx({path})")
+    try:
+        n = m.nnz
+        raw = np.ctypeslib.as_array(C.cast(m.data, C.POINTER(C.c_int)), (3 * n,)) if n else np.zeros(0, np.int32)
+        t = raw.reshape(n, 3).copy() if n else np.zeros((0, 3), np.int32)
+        vals = t[:, 2].view(np.float32).copy()
+        return m.num_rows, m.num_cols, t[:, 0].astype(np.int64), t[:, 1].astype(np.int64), vals
+    finally:
+        L.freeCOO(C.byref(m))
 
 
 def version() -> str:

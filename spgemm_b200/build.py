@@ -28,6 +28,7 @@ SOURCES = [
     "api.cu",
     "legacy_mm.cu",
     "host_coo.cpp",
+    "host_mtx.cpp",
     "host_cm.cpp",
     "host_legacy.cpp",
     "legacy_spgemm.cu",

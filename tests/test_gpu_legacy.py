@@ -75,3 +75,56 @@ def test_unsorted_coo_reported(outer_bin, tmp_path):
     assert L.spgemm_legacy_status() == 1
     L.spgemm_set_exit_on_error(1)
     L.spgemm_set_verbose(1)
+
+
+def _coo_of(M, col_major):
+    """Triplets of host CSR M sorted as the protocol wants: by (column, row)
+    for the COL_MAJOR operand A, by (row, column) for the ROW_MAJOR B."""
+    r = np.repeat(np.arange(M.rows), np.diff(M.rowptr)).astype(np.int64)
+    c = M.col.astype(np.int64)
+    order = np.lexsort((r, c)) if col_major else np.lexsort((c, r))
+    trip = (sg.Triplet * max(M.nnz, 1))()
+    for t, k in enumerate(order):
+        trip[t] = (int(r[k]), int(c[k]), float(M.val[k]))
+    return trip
+
+
+def test_dense_chunk_product_matches_oracle():
+    """cudaDCGEMM (dense-chunk strategy: rows in dense column windows) right
+    after cudaInitGEMM gives the oracle's C, and leaves the handle's tuning
+    in place for a following cudaBinGEMM + cudaMergeGEMM product."""
+    import ctypes as C
+    L = sg.lib()
+    L.spgemm_set_verbose(0)
+    try:
+        A = W.rmat(12, 12, 8, values="sym")
+        B = W.rmat(12, 10, 9, values="sym")
+        ta, tb = _coo_of(A, True), _coo_of(B, False)
+        ca = sg.COO(C.cast(ta, C.POINTER(sg.Triplet)), A.nnz, A.cols, A.rows, sg.COL_MAJOR)
+        cb = sg.COO(C.cast(tb, C.POINTER(sg.Triplet)), B.nnz, B.cols, B.rows, sg.ROW_MAJOR)
+        Ah = L.cudaCOO2CM(ca)
+        Bh = L.cudaCOO2CM(cb)
+        a = A.to_csc()
+        ref = oracle.spgemm(A.rows, B.cols, a.colptr, a.rowidx, a.val, B.rowptr, B.col, B.val,
+                            stats=True)
+        L.spgemm_get_result.restype = C.c_int
+        for dense in (True, False):
+            Cm = L.cudaInitGEMM(Ah, Bh)
+            if dense:
+                L.cudaDCGEMM(Ah, Bh, Cm)
+            else:
+                L.cudaBinGEMM(Ah, Bh, Cm)
+                L.cudaMergeGEMM(Cm)
+            R = sg.CM()
+            assert L.spgemm_get_result(C.byref(R)) == 0
+            ptr = np.ctypeslib.as_array(R.ptr, (R.num_rows + 1,)).copy()
+            col = np.ctypeslib.as_array(R.idx, (max(R.nnz, 1),))[:R.nnz].copy()
+            val = np.ctypeslib.as_array(R.val, (max(R.nnz, 1),))[:R.nnz].copy()
+            L.cmFree(C.byref(R))
+            from helpers import assert_structure_equal, assert_values_close, plain_tolerance
+            assert_structure_equal(ptr, col, ref["rowptr"], ref["col"])
+            assert_values_close(val, ref, plain_tolerance(ref))
+        for M in (Ah, Bh):
+            L.cmFree(C.byref(M))
+    finally:
+        L.spgemm_set_verbose(1)
