@@ -32,9 +32,11 @@ struct DenseChunk
 };
 typedef struct DenseChunk dc;
 
-/* Sorted COO -> CSC (type COL_MAJOR, becomes operand A) or CSR
- * (ROW_MAJOR, becomes operand B) on the GPU; returns a host copy whose
- * arrays are malloc'd. Replaces reference src/mm.cu:65-136. */
+/* COO -> CSC (type COL_MAJOR, becomes operand A) or CSR (ROW_MAJOR,
+ * becomes operand B) on the GPU; returns a host copy whose arrays are
+ * malloc'd. Input sorted by sortCOO (the reference protocol) takes a direct
+ * split and scan; any other order is sorted on the device first (the
+ * reference requires the host sort). Replaces reference src/mm.cu:65-136. */
 cm cudaCOO2CM(coo mat);
 /* Row analysis of A*B: returns C's shape with nnz = the number of
  * intermediate products P (clamped to INT_MAX; the exact 64-bit value is

@@ -190,6 +190,22 @@ int spgemm_reset_kernel_times(spgemm_handle_t handle);
 int spgemm_get_kernel_times(spgemm_handle_t handle, char* names, int names_len,
                             double* ms, long long* launches, int max_kernels);
 
+/* COO -> compressed on the device, triplets in any order: the conversion of
+ * cudaCOO2CM (reference src/mm.cu:65-136) without the host sortCOO the
+ * reference's protocol needs first (src/coo.cpp:73-79). d_triplets: nnz
+ * device triplets; type ROW_MAJOR -> CSR (d_ptr[num_rows + 1]), COL_MAJOR ->
+ * CSC (d_ptr[num_cols + 1]); d_idx / d_val [nnz]. Minor indices come out
+ * ascending within each row (column), entries with equal indices in input
+ * order. Counting sort on the major index, then per-row sorts in shared
+ * memory (warp, block, or block-merged runs for rows above 8192 entries).
+ * Uses handle-owned scratch (about 16 bytes per entry) and synchronises the
+ * handle's stream once. An index outside its dimension: SPGEMM_ERR_INVALID
+ * (the output then omits those entries). cudaCOO2CM takes this path by
+ * itself when its input is not sorted. */
+int spgemm_coo_to_cm(spgemm_handle_t handle, const triplet* d_triplets, int nnz,
+                     int num_rows, int num_cols, int type, int* d_ptr, int* d_idx,
+                     float* d_val);
+
 /* Value-preserving Matrix-Market reader. The reference's readMTX
  * (src/coo.cpp:110-173, kept unchanged in coo.h) forces every value to 1.1,
  * reads the first size token as the column count and misparses pattern

@@ -117,6 +117,7 @@ def lib():
         L.spgemm_batch_copy_result.argtypes = [vp, C.c_int, ip, ip, fp]
         L.spgemm_batch_copy_all.argtypes = [vp, vp, vp, vp]
         L.spgemm_read_mtx.argtypes = [C.POINTER(COO), C.c_char_p]
+        L.spgemm_coo_to_cm.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp, vp, vp]
         L.cmFree.argtypes = [C.POINTER(CM)]
         L.cudaCOO2CM.restype = CM
         L.cudaCOO2CM.argtypes = [COO]
@@ -311,6 +312,14 @@ class Handle:
         out = CM()
         self._check(lib().spgemm_multiply(self._h, A, B, C.byref(out)))
         return out
+
+    def coo_to_cm(self, d_triplets: int, nnz: int, rows: int, cols: int, kind: int,
+                  d_ptr: int, d_idx: int, d_val: int) -> None:
+        """Device triplets in any order to CSR (ROW_MAJOR) or CSC (COL_MAJOR)
+        in caller device arrays (spgemm_coo_to_cm)."""
+        self._check(lib().spgemm_coo_to_cm(self._h, C.c_void_p(d_triplets), nnz, rows, cols, kind,
+                                           C.c_void_p(d_ptr), C.c_void_p(d_idx),
+                                           C.c_void_p(d_val)))
 
     # -- batched products (device operands) --------------------------------
     def batch_plan(self, A_list, B_list) -> int:

@@ -25,6 +25,7 @@ LIB = PKG / "libspgemm_b200.so"
 SOURCES = [
     "engine.cu",
     "batch.cu",
+    "coo_sort.cu",
     "api.cu",
     "legacy_mm.cu",
     "host_coo.cpp",

@@ -173,6 +173,23 @@ int spgemm_batch_copy_all(spgemm_handle_t h, int* c_rowptr, int* c_colidx, float
   return h->batch.copy_all(h->eng, c_rowptr, c_colidx, c_val);
 }
 
+int spgemm_coo_to_cm(spgemm_handle_t h, const triplet* d_triplets, int nnz, int num_rows,
+                     int num_cols, int type, int* d_ptr, int* d_idx, float* d_val) {
+  if (!h) return SPGEMM_ERR_INVALID;
+  sg::Engine& E = h->eng;
+  const bool row_major = type == ROW_MAJOR;
+  const int n_major = row_major ? num_rows : num_cols;
+  const int n_minor = row_major ? num_cols : num_rows;
+  if (nnz < 0 || n_major < 0 || n_minor < 0 || !d_ptr || (nnz > 0 && (!d_triplets || !d_idx || !d_val)))
+    return E.fail(SPGEMM_ERR_INVALID, "coo_to_cm: invalid argument");
+  unsigned flags = 0;
+  cudaError_t e = sg::coo_compress(d_triplets, nnz, row_major, n_major, n_minor, d_ptr, d_idx,
+                                   d_val, h->coo_scratch, h->coo_scan, &flags, E.stream());
+  if (e != cudaSuccess) return E.cuda_fail(e, "coo_to_cm");
+  if (flags & 1u) return E.fail(SPGEMM_ERR_INVALID, "coo_to_cm: index outside the dimensions");
+  return SPGEMM_OK;
+}
+
 int spgemm_get_stats(spgemm_handle_t h, spgemm_stats* out) {
   if (!h || !out) return SPGEMM_ERR_INVALID;
   memset(out, 0, sizeof(*out));

@@ -8,4 +8,10 @@
 struct spgemm_context {
   sg::Engine eng;
   sg::Batch batch;
+  sg::DevBuf coo_scratch, coo_scan;  // spgemm_coo_to_cm workspace
+
+  ~spgemm_context() {
+    coo_scratch.release();
+    coo_scan.release();
+  }
 };

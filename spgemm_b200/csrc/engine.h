@@ -186,6 +186,16 @@ class Engine {
 
 Tuning default_tuning();
 
+// Triplets in any order (device) to compressed form: row_major -> CSR over
+// rows, else CSC over columns; minor indices ascending within each major
+// index, entries with equal indices in input order. ptr[n_major + 1],
+// idx/val[nnz]. Entries with an index outside its dimension are left out and
+// set bit 0 of *flags_host (when non-null the call synchronises `stream` to
+// read it).
+cudaError_t coo_compress(const triplet* t, int nnz, bool row_major, int n_major, int n_minor,
+                         int* ptr, int* idx, float* val, DevBuf& scratch, DevBuf& scan_tmp,
+                         unsigned* flags_host, cudaStream_t stream);
+
 // Exclusive scan of n int32 counts into n+1 int32 pointers on `stream`.
 // `tmp` is scratch (grown as needed); `total_dev` receives the sum (int64).
 cudaError_t scan_counts_to_ptr32(const int* cnt, int n, int* ptr, DevBuf& tmp,

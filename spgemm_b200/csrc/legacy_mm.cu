@@ -27,7 +27,7 @@ int g_status = SPGEMM_OK;
 // src/mm.cu:19-25).
 sg::DevBuf g_a_ptr, g_a_idx, g_a_val;  // A: CSC
 sg::DevBuf g_b_ptr, g_b_idx, g_b_val;  // B: CSR
-sg::DevBuf g_tmp_triplets, g_tmp_cnt, g_tmp_ptr64, g_tmp_flag;
+sg::DevBuf g_tmp_triplets, g_tmp_cnt, g_tmp_ptr64, g_tmp_flag, g_tmp_sort;
 cm g_A_dev, g_B_dev;
 bool g_have_a = false, g_have_b = false, g_have_c = false;
 
@@ -173,9 +173,24 @@ cm cudaCOO2CM(coo mat) {
       return ret;
     }
     if (flags & 2u) {
-      LEGACY_FAIL(SPGEMM_ERR_INVALID,
-                  "cudaCOO2CM: triplets not sorted (call sortCOO first, as the protocol requires)");
-      return ret;
+      // Not in the protocol's order (sortCOO skipped): sort on the device
+      // instead of on the host. Entries with equal indices keep their order.
+      unsigned f2 = 0;
+      e = sg::coo_compress(g_tmp_triplets.as<triplet>(), mat.nnz, row_major, n_major, n_minor,
+                           dptr.as<int>(), didx.as<int>(), dval.as<float>(), g_tmp_sort,
+                           g_tmp_ptr64, &f2, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ret.ptr, dptr.ptr, sizeof(int) * ((size_t)n_major + 1),
+                            cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && nnz)
+        e = cudaMemcpyAsync(ret.idx, didx.ptr, sizeof(int) * nnz, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && nnz)
+        e = cudaMemcpyAsync(ret.val, dval.ptr, sizeof(float) * nnz, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) {
+        LEGACY_FAIL(SPGEMM_ERR_CUDA, cudaGetErrorString(e));
+        return ret;
+      }
     }
   }
   cm dev = ret;

@@ -62,19 +62,39 @@ def test_outer_driver_matches_oracle(outer_bin, tmp_path, scale):
     assert (np.abs(data[:, 2] - ref["val"]) <= tol).all()
 
 
-def test_unsorted_coo_reported(outer_bin, tmp_path):
-    """cudaCOO2CM on triplets that skip sortCOO: the protocol requires
-    sorted input; the library reports it instead of building a bad CSC."""
+def test_unsorted_coo_is_sorted_on_the_device():
+    """cudaCOO2CM on triplets that skip sortCOO: the reference protocol
+    requires sorted input; the library sorts on the device and returns the
+    same compressed matrix as for the sorted triplets."""
     import ctypes as C
     L = sg.lib()
-    L.spgemm_set_exit_on_error(0)
     L.spgemm_set_verbose(0)
-    trip = (sg.Triplet * 3)((2, 0, 1.0), (0, 1, 2.0), (1, 0, 3.0))
-    coo = sg.COO(C.cast(trip, C.POINTER(sg.Triplet)), 3, 3, 3, sg.ROW_MAJOR)
-    L.cudaCOO2CM(coo)
-    assert L.spgemm_legacy_status() == 1
-    L.spgemm_set_exit_on_error(1)
-    L.spgemm_set_verbose(1)
+    try:
+        rng = np.random.default_rng(4)
+        n = 300
+        r = rng.integers(0, n, 4000)
+        c = rng.integers(0, n, 4000)
+        v = rng.uniform(-1, 1, 4000).astype(np.float32)
+        key = np.unique(r * n + c)  # distinct positions
+        r, c, v = key // n, key % n, v[:len(key)]
+        perm = rng.permutation(len(key))
+        for major in ("row", "col"):
+            kind = sg.ROW_MAJOR if major == "row" else sg.COL_MAJOR
+            order = np.lexsort((c, r)) if major == "row" else np.lexsort((r, c))
+            outs = []
+            for idx in (order, perm):
+                trip = (sg.Triplet * len(idx))(*[(int(r[k]), int(c[k]), float(v[k])) for k in idx])
+                coo = sg.COO(C.cast(trip, C.POINTER(sg.Triplet)), len(idx), n, n, kind)
+                M = L.cudaCOO2CM(coo)
+                assert L.spgemm_legacy_status() == 0
+                outs.append([np.ctypeslib.as_array(M.ptr, (n + 1,)).copy(),
+                             np.ctypeslib.as_array(M.idx, (M.nnz,)).copy(),
+                             np.ctypeslib.as_array(M.val, (M.nnz,)).copy()])
+                L.cmFree(C.byref(M))
+            for a, b in zip(*outs):
+                assert np.array_equal(a, b)
+    finally:
+        L.spgemm_set_verbose(1)
 
 
 def _coo_of(M, col_major):
