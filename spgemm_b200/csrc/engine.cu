@@ -512,12 +512,13 @@ int Engine::launch_fused() {
     const int b = L - 11 + FB_BLOCK0;                                                          \
     const int bound = fb_counts_[b] + (L == 13 ? overflow_bound : 0);                          \
     if (bound > 0) {                                                                           \
-      const size_t smem = (size_t(1) << L) * (VB + 4) + (NT / 32) * SEG_SCRATCH_BYTES;         \
+      const size_t smem = (size_t(1) << L) * (VB + 5) + (NT / 32) * SEG_SCRATCH_BYTES;         \
       SG_CK(smem_attr(k_fused_block<L, NT, MODE>, smem), "smem attr k_fused_block");           \
       prof_begin("k_fused_block<" #L ">");                                                     \
       k_fused_block<L, NT, MODE><<<blocks_for(bound, 1, (long long)sms_ * 8), NT, smem,         \
                                    stream_>>>(op, rows + (size_t)b * m, &dc->fb_count[b],      \
-                                              row_p, toff, c_cnt, t_col, t_val, status);       \
+                                              row_p, toff, row_span_.as<int2>(), c_cnt, t_col, \
+                                              t_val, status);                                  \
       SG_LAUNCHED("k_fused_block");                                                            \
     }                                                                                          \
   }

@@ -736,9 +736,11 @@ __device__ __forceinline__ int long_slot(const uint2* dir, int lo, int col) {
 }
 
 // Value-pass functors of the bitmap slices: accumulate into the output slot
-// and record the slot's column (every product of a column stores the same
-// index), so the write-out copies columns like values instead of expanding
-// the directory.
+// and record the slot's column, so the write-out copies columns like values
+// instead of expanding the directory. Slots start at +0.0; the plain form
+// stores the column when its add found the slot still at +0.0 (the first
+// product of the column does, so every slot gets its column; a later store
+// after an exact cancellation writes the same index again).
 struct LongValPlain {
   const uint2* dir;
   float* vals;
@@ -748,8 +750,8 @@ struct LongValPlain {
   __device__ __forceinline__ void operator()(int col, float a, float b) {
     if ((unsigned)(col - lo) < width) {
       const int s = long_slot(dir, lo, col);
-      atomicAdd(vals + s, __fmul_rn(a, b));
-      cols[s] = col;
+      const float old = atomicAdd(vals + s, __fmul_rn(a, b));
+      if (__float_as_uint(old) == 0u) cols[s] = col;
     }
   }
 };

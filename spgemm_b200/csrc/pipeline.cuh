@@ -409,8 +409,8 @@ template <int LOG2T, int NT, int MODE>
 __global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 4)
 k_fused_block(Operands op, const int* __restrict__ rows, const int* __restrict__ nrows_p,
               const long long* __restrict__ row_p, const long long* __restrict__ toff,
-              int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
-              unsigned* status) {
+              const int2* __restrict__ row_span, int* __restrict__ c_cnt,
+              int* __restrict__ t_col, float* __restrict__ t_val, unsigned* status) {
   constexpr int T = 1 << LOG2T;
   constexpr int NW = NT / 32;
   constexpr int PER = T / NT;  // slots per thread in the compaction
@@ -421,6 +421,10 @@ k_fused_block(Operands op, const int* __restrict__ rows, const int* __restrict__
   V* vals = reinterpret_cast<V*>(smem);
   unsigned* keys = reinterpret_cast<unsigned*>(smem + T * sizeof(V));
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * (sizeof(V) + 4)) + warp;
+  constexpr int NB = T / 4;         // sort buckets
+  constexpr int PB = NB / NT;       // bucket counters per thread in the scan
+  int* bucket = reinterpret_cast<int*>(smem + T * (sizeof(V) + 4) + NW * sizeof(SegScratch));
+  __shared__ int bucket_max;
   const int nrows = *nrows_p;
   for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = rows[r];
@@ -452,20 +456,92 @@ k_fused_block(Operands op, const int* __restrict__ rows, const int* __restrict__
     long long o64;
     long long pos = block_excl_scan64(mine, scan_shm, o64);
     const int o = (int)o64;
+    const int pos0 = (int)pos;
 #pragma unroll
     for (int q = 0; q < PER; ++q)
       if (k[q] != EMPTY_KEY) { keys[pos] = k[q]; vals[pos] = v[q]; ++pos; }
     __syncthreads();
     int n2 = 1;
     while (n2 < o) n2 <<= 1;
-    for (int t = o + threadIdx.x; t < n2; t += NT) keys[t] = EMPTY_KEY;
-    __syncthreads();
-    bitonic_sort_kv_rt(keys, vals, n2, threadIdx.x, NT, BlockSync());
     const long long base = toff[i];
-    for (int t = threadIdx.x; t < o; t += NT) {
-      t_col[base + t] = (int)keys[t];
-      if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
-      else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+    const int2 sp = row_span[i];
+    const unsigned lo = (unsigned)(sp.x & ~31);
+    const unsigned span = (unsigned)(sp.y + 1) - lo;
+    bool sorted_packed = false;
+    if (o > 256 && span <= (1u << (32 - LOG2T))) {
+      // packed keys (column - lo) << LOG2T | slot, held in registers; the
+      // values stay in their compacted slots. Bucket pass on the column
+      // offset's top bits + per-bucket insertion, as in k_fused_warp.
+      unsigned pk[PER];
+      int j = pos0;
+#pragma unroll
+      for (int q = 0; q < PER; ++q)
+        pk[q] = k[q] != EMPTY_KEY ? ((k[q] - lo) << LOG2T) | (unsigned)(j++) : EMPTY_KEY;
+      const int bits = 32 - __clz(span > 1 ? span - 1 : 1);
+      const int shift = bits > LOG2T - 2 ? bits - (LOG2T - 2) : 0;
+      for (int t = threadIdx.x; t < NB; t += NT) bucket[t] = 0;
+      if (threadIdx.x == 0) bucket_max = 0;
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < PER; ++q)
+        if (pk[q] != EMPTY_KEY) atomicAdd(&bucket[(pk[q] >> LOG2T) >> shift], 1);
+      __syncthreads();
+      int cnt[PB], sum = 0, mx = 0;
+#pragma unroll
+      for (int q = 0; q < PB; ++q) {
+        cnt[q] = bucket[threadIdx.x * PB + q];
+        sum += cnt[q];
+        mx = max(mx, cnt[q]);
+      }
+      if (mx > BUCKET_MAX) atomicMax(&bucket_max, mx);
+      long long tot;
+      long long run = block_excl_scan64(sum, scan_shm, tot);  // ends with a barrier
+      if (bucket_max == 0) {
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
+          bucket[threadIdx.x * PB + q] = (int)run;
+          run += cnt[q];
+        }
+        __syncthreads();
+        // every key is in registers: scatter into the key array by bucket
+#pragma unroll
+        for (int q = 0; q < PER; ++q)
+          if (pk[q] != EMPTY_KEY) keys[atomicAdd(&bucket[(pk[q] >> LOG2T) >> shift], 1)] = pk[q];
+        __syncthreads();
+        for (int b = threadIdx.x; b < NB; b += NT) {
+          const int s0 = b ? bucket[b - 1] : 0, s1 = bucket[b];
+          for (int x = s0 + 1; x < s1; ++x) {
+            const unsigned kv = keys[x];
+            int y = x - 1;
+            while (y >= s0 && keys[y] > kv) {
+              keys[y + 1] = keys[y];
+              --y;
+            }
+            keys[y + 1] = kv;
+          }
+        }
+        __syncthreads();
+        sorted_packed = true;
+      }
+      // crowded buckets: the key/value bitonic sort below
+    }
+    if (sorted_packed) {
+      for (int t = threadIdx.x; t < o; t += NT) {
+        const unsigned p = keys[t];
+        const int slot = (int)(p & (T - 1));
+        t_col[base + t] = (int)(lo + (p >> LOG2T));
+        if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[slot]);
+        else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[slot]);
+      }
+    } else {
+      for (int t = o + threadIdx.x; t < n2; t += NT) keys[t] = EMPTY_KEY;
+      __syncthreads();
+      bitonic_sort_kv_rt(keys, vals, n2, threadIdx.x, NT, BlockSync());
+      for (int t = threadIdx.x; t < o; t += NT) {
+        t_col[base + t] = (int)keys[t];
+        if (MODE == 0) t_val[base + t] = finalize_value(reinterpret_cast<float*>(vals)[t]);
+        else t_val[base + t] = finalize_value(reinterpret_cast<float2*>(vals)[t]);
+      }
     }
     if (threadIdx.x == 0) c_cnt[i] = o;
     __syncthreads();
