@@ -24,7 +24,7 @@ SEARCH = [
     ("warp_p_max", [1024, 2048, 4096]),
     ("warp_cap_max", [512, 1024, 2048]),
     ("long_p", [2048, 4096]),
-    ("mid_cols", [1 << 16, 1 << 18]),
+    ("mid_cols", [0, 1 << 16, 1 << 18]),
 ]
 
 DEFAULT_CACHE = Path(os.environ.get("SPGEMM_B200_TUNE_CACHE",
