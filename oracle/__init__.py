@@ -1,8 +1,8 @@
 """CPU oracle for the SpGEMM path -- test infrastructure only.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` may import this package, and only as the checker / the timed CPU
-baseline. The product path (``spgemm_b200``) never imports it.
+``bench.py`` may import this package, and only to check results against / as
+the timed CPU baseline. The product path (``spgemm_b200``) never imports it.
 
 ``liboracle.so`` is the C restatement in ``spgemm_oracle.c`` (see its header
 for the reference lines it follows); ``_ref/libref_host.so`` is the

@@ -1,7 +1,7 @@
 /* CPU oracle for the SpGEMM path -- TEST INFRASTRUCTURE ONLY.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
- * load this library, and only as the checker / the timed CPU baseline. The
+ * load this library, and only to check results / as the timed CPU baseline. The
  * product path (spgemm_b200) never calls it.
  *
  * It restates the algorithm of the reference's live engine, src/mm.cu:

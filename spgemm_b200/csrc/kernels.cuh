@@ -10,15 +10,20 @@
 // each own a column slice. Partials never touch HBM.
 //
 // Pipeline (kernel names):
+//   k_validate        index ranges and sortedness of the inputs
 //   k_transpose_hist / k_transpose_scatter  A CSC -> CSR (row-wise expansion)
-//   k_row_analysis    P_i per row, flattened offsets, symbolic binning
-//   k_sym_warp/block  exact nnz of short/mid rows via shared-memory hashing
+//   k_row_analysis    P_i per row, flattened offsets, column spans, bins
+//   k_fused_warp/block  rows of at most long_p products in one pass: hash
+//                     accumulate, sort, row written to a temporary buffer
+//   k_num_long<.,512,sparse> as k_fused_mid  the same for rows whose column
+//                     span fits a bitmap (two passes over the row on chip)
 //   k_sym_long        exact nnz of long rows via a shared-memory bitmap
 //   k_scan_*          row pointers of C
 //   k_num_bin         numeric binning + column slicing of long rows
-//   k_num_warp/block  numeric hash merge + bitonic sort -> sorted CSR rows
-//   k_num_long        numeric bitmap-rank merge (a counting sort on the
+//   k_copy_fused      fused rows from the temporary buffer into C
+//   k_num_long        long rows: bitmap-rank merge (a counting sort on the
 //                     column) -> sorted CSR slices
+//   k_num_block       long rows with few outputs: block hash + sort
 #pragma once
 
 #include "common.cuh"
