@@ -535,7 +535,7 @@ int Engine::numeric_values(int* c_col, float* c_val) {
   if (nnz_c_ > 0 && (!c_col || !c_val)) return fail(1, "null output pointer");
   if (m_ > 0 && temp_total_ > 0) {
     prof_begin("k_copy_fused");
-    k_copy_fused<<<blocks_for((long long)m_ * 32, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+    k_copy_fused<<<blocks_for((long long)m_, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
         m_, tcap_.as<int>(), toff_.as<long long>(), c_cnt_.as<int>(), c_rowptr64_.as<long long>(),
         t_col_.as<int>(), t_val_.as<float>(), c_col, c_val);
     SG_LAUNCHED("k_copy_fused");

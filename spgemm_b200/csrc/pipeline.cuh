@@ -741,15 +741,42 @@ k_copy_fused(int m, const int* __restrict__ tcap, const long long* __restrict__ 
              const int* __restrict__ c_cnt, const long long* __restrict__ c_rowptr,
              const int* __restrict__ t_col, const float* __restrict__ t_val,
              int* __restrict__ c_col, float* __restrict__ c_val) {
+  // A warp takes 32 rows at a time: each lane loads one row's length and
+  // offsets (so the 32 rows' loads are in flight together), then the warp
+  // copies the rows one after the other, two entries per lane per step.
   const int lane = threadIdx.x & 31;
-  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < m;
-       i += (gridDim.x * blockDim.x) >> 5) {
-    if (tcap[i] == 0) continue;
-    const int n = c_cnt[i];
-    const long long src = toff[i], dst = c_rowptr[i];
-    for (int t = lane; t < n; t += 32) {
-      __stcs(c_col + dst + t, __ldcs(t_col + src + t));
-      __stcs(c_val + dst + t, __ldcs(t_val + src + t));
+  const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < m;
+       i0 += warps * 32) {
+    const long long i = i0 + lane;
+    int n = 0;
+    long long src = 0, dst = 0;
+    if (i < m && tcap[i] != 0) {
+      n = c_cnt[i];
+      src = toff[i];
+      dst = c_rowptr[i];
+    }
+    for (int r = 0; r < 32; ++r) {
+      const int nr = __shfl_sync(FULL, n, r);
+      if (nr == 0) continue;  // warp-uniform
+      const long long s = __shfl_sync(FULL, src, r), d = __shfl_sync(FULL, dst, r);
+      for (int t = lane; t < nr; t += 64) {
+        const bool two = t + 32 < nr;
+        const int c0 = __ldcs(t_col + s + t);
+        const float v0 = __ldcs(t_val + s + t);
+        int c1 = 0;
+        float v1 = 0.f;
+        if (two) {
+          c1 = __ldcs(t_col + s + t + 32);
+          v1 = __ldcs(t_val + s + t + 32);
+        }
+        __stcs(c_col + d + t, c0);
+        __stcs(c_val + d + t, v0);
+        if (two) {
+          __stcs(c_col + d + t + 32, c1);
+          __stcs(c_val + d + t + 32, v1);
+        }
+      }
     }
   }
 }
