@@ -102,10 +102,14 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
   __shared__ int hist[FB_COUNT], base[FB_COUNT];
   __shared__ int rowbin[RA_ROWS], rowrank[RA_ROWS];
   __shared__ unsigned long long block_p;
+  __shared__ int block_max_len;  // longest A row of the block (one global atomic per block)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int row0 = blockIdx.x * RA_ROWS;
   if (threadIdx.x < FB_COUNT) hist[threadIdx.x] = 0;
-  if (threadIdx.x == 0) block_p = 0;
+  if (threadIdx.x == 0) {
+    block_p = 0;
+    block_max_len = 0;
+  }
   __syncthreads();
   for (int lr = warp; lr < RA_ROWS; lr += RA_THREADS / 32) {
     const int i = row0 + lr;
@@ -146,7 +150,7 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
       hi = max(hi, __shfl_xor_sync(FULL, hi, d));
     }
     if (lane == 0) {
-      if (re - rs > 0) atomicMax(max_row_len, re - rs);
+      if (re - rs > 0) atomicMax(&block_max_len, re - rs);
       const int span = acc > 0 ? hi + 1 - lo : 0;
       row_span[i] = acc > 0 ? make_int2(lo, hi) : make_int2(0, -1);
       row_p[i] = acc;
@@ -163,7 +167,10 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
   __syncthreads();
   if (threadIdx.x < FB_COUNT && hist[threadIdx.x])
     base[threadIdx.x] = atomicAdd(fb_count + threadIdx.x, hist[threadIdx.x]);
-  if (threadIdx.x == 0) atomicAdd(p_total, block_p);
+  if (threadIdx.x == 0) {
+    atomicAdd(p_total, block_p);
+    if (block_max_len > 0) atomicMax(max_row_len, block_max_len);
+  }
   __syncthreads();
   for (int lr = threadIdx.x; lr < RA_ROWS; lr += RA_THREADS) {
     const int b = rowbin[lr];
