@@ -128,3 +128,52 @@ def spgemm(m, n, a_colptr, a_rowidx, a_val, b_rowptr, b_colidx, b_val, rows=None
         return out
     finally:
         lib().oracle_free(r)
+
+
+REF_MM_PATH = HERE / "_ref" / "ref_mm"
+
+
+def ref_available() -> bool:
+    """True when _ref/ref_mm (the reference's own src/mm.cu built for the CPU) exists."""
+    return REF_MM_PATH.exists()
+
+
+def ref_multiply(m, k, n, a_row, a_col, a_val, b_row, b_col, b_val, workdir):
+    """C = A*B by the reference's own engine (src/mm.cu) run on the CPU.
+
+    A (m x k) and B (k x n, square: n == k) are given as COO triplets in any
+    order; the driver sorts them with the reference's sortCOO. Returns a dict:
+    ``p`` and ``nnzc`` / ``nnzcf`` as the reference prints them
+    (src/mm.cu:181, :449), and per row the merged bucket as the reference
+    leaves it in its module globals: ``base`` (c_ptr_base), ``cnt``
+    (c_ptr_nnz), ``idx`` / ``val`` (c_idx / c_val, columns in merge order).
+    """
+    if not ref_available():
+        raise FileNotFoundError(f"{REF_MM_PATH} is not built (make -C oracle REF=...)")
+    workdir = Path(workdir)
+    inp, out = workdir / "ref_in.bin", workdir / "ref_out.bin"
+    trip = np.dtype([("r", np.int32), ("c", np.int32), ("v", np.float32)])
+
+    def pack(r, c, v):
+        t = np.empty(len(r), trip)
+        t["r"], t["c"], t["v"] = r, c, v
+        return t.tobytes()
+
+    with open(inp, "wb") as f:
+        f.write(np.array([m, k, n, len(a_row), len(b_row)], np.int32).tobytes())
+        f.write(pack(a_row, a_col, a_val))
+        f.write(pack(b_row, b_col, b_val))
+    r = subprocess.run([str(REF_MM_PATH), str(inp), str(out)], capture_output=True, text=True,
+                       timeout=600)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_mm failed ({r.returncode}): {r.stderr[-2000:]}")
+    lines = [ln.split() for ln in r.stdout.splitlines() if ln.strip()]
+    raw = np.fromfile(out, dtype=np.int32)
+    mm, p = int(raw[0]), int(raw[1])
+    o = 2
+    base = raw[o:o + mm + 1]; o += mm + 1
+    cnt = raw[o:o + mm]; o += mm
+    idx = raw[o:o + p]; o += p
+    val = raw[o:o + p].view(np.float32)
+    return {"p": int(lines[0][0]), "p_again": int(lines[0][1]), "nnzc": int(lines[1][0]),
+            "nnzcf": int(lines[1][1]), "base": base, "cnt": cnt, "idx": idx, "val": val}
