@@ -27,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "../../include/spGEMM.h"
@@ -376,15 +377,95 @@ int cudaPass2(void) {
   return nnzC;
 }
 
+// The workload tables describe a decomposition of the products into per-k
+// outer products (wlt: one record per k, lib/wlt.h:10-23) and, with `cheat`,
+// into 2-D tiles of heavy outer products (wlt_cheat: first A entry ridx and
+// first B entry cidx of each tile, the pairs calcInterDom works on,
+// src/spGEMM.cu:543-589). C = A*B does not depend on how the products are
+// decomposed, and the engine derives its own per-row decomposition, so the
+// tables steer nothing here; but a table that does not describe these
+// operands means the caller's picture of the product is wrong, so it is
+// checked and rejected. An empty table (null data or zero records) is not
+// checked. Returns an empty string when the tables are consistent.
+static std::string check_wlt(const csc& A, const csr& B, const wlt& W) {
+  if (!W.data || W.threadblocks <= 0) return "";
+  const int n = A.n;
+  std::vector<char> seen((size_t)n, 0);
+  long long total = 0;
+  for (int t = 0; t < W.threadblocks; ++t) {
+    const wltData& d = W.data[t];
+    if (d.idx < 0 || d.idx >= n) return "wlt record " + std::to_string(t) + ": k out of range";
+    if (seen[d.idx]) return "wlt record " + std::to_string(t) + ": k listed twice";
+    seen[d.idx] = 1;
+    const int ca = A.header[d.idx + 1] - A.header[d.idx];
+    const int rb = B.header[d.idx + 1] - B.header[d.idx];
+    if (d.num_of_col_elements != ca || d.num_of_row_elements != rb)
+      return "wlt record " + std::to_string(t) + ": element counts differ from the operands";
+    total += (long long)ca * rb;
+  }
+  for (int k = 0; k < n; ++k)
+    if (!seen[k] && (long long)(A.header[k + 1] - A.header[k]) * (B.header[k + 1] - B.header[k]) > 0)
+      return "wlt: the outer product of k = " + std::to_string(k) + " is missing";
+  if (total <= INT_MAX && W.workloads != (int)total) return "wlt: workloads differs from the product count";
+  return "";
+}
+
+// Every tile must lie inside one outer product, and the tiles of an outer
+// product must cover it exactly (their areas add up to nnz(A(:,k)) *
+// nnz(B(k,:)) and no two tiles overlap).
+static std::string check_wlt_cheat(const csc& A, const csr& B, const wlt_cheat& T) {
+  if (!T.data || T.threadblocks <= 0) return "";
+  struct Tile { int k, r0, r1, c0, c1; };
+  std::vector<Tile> tiles;
+  tiles.reserve((size_t)T.threadblocks);
+  for (int t = 0; t < T.threadblocks; ++t) {
+    const wltData_cheat& d = T.data[t];
+    if (d.ridx < 0 || d.ridx >= A.e || d.num_of_col_elements <= 0 || d.num_of_row_elements <= 0)
+      return "wlt_cheat tile " + std::to_string(t) + ": empty or out of range";
+    // column k of A holding entry ridx
+    const int k = (int)(std::upper_bound(A.header, A.header + A.n + 1, d.ridx) - A.header) - 1;
+    if (k < 0 || k >= A.n || d.ridx + d.num_of_col_elements > A.header[k + 1])
+      return "wlt_cheat tile " + std::to_string(t) + ": A entries leave column k";
+    if (d.cidx < B.header[k] || d.cidx + d.num_of_row_elements > B.header[k + 1])
+      return "wlt_cheat tile " + std::to_string(t) + ": B entries leave row k";
+    tiles.push_back(Tile{k, d.ridx, d.ridx + d.num_of_col_elements, d.cidx,
+                         d.cidx + d.num_of_row_elements});
+  }
+  std::sort(tiles.begin(), tiles.end(), [](const Tile& a, const Tile& b) {
+    return a.k != b.k ? a.k < b.k : (a.r0 != b.r0 ? a.r0 < b.r0 : a.c0 < b.c0);
+  });
+  for (size_t s = 0; s < tiles.size();) {
+    size_t e = s;
+    long long area = 0;
+    const int k = tiles[s].k;
+    while (e < tiles.size() && tiles[e].k == k) {
+      area += (long long)(tiles[e].r1 - tiles[e].r0) * (tiles[e].c1 - tiles[e].c0);
+      ++e;
+    }
+    const long long full = (long long)(A.header[k + 1] - A.header[k]) * (B.header[k + 1] - B.header[k]);
+    if (area != full) return "wlt_cheat: the tiles of k = " + std::to_string(k) + " do not cover it";
+    for (size_t x = s; x < e; ++x)  // pairwise overlap test inside one outer product
+      for (size_t y = x + 1; y < e && tiles[y].r0 < tiles[x].r1; ++y)
+        if (tiles[y].c0 < tiles[x].c1 && tiles[x].c0 < tiles[y].c1)
+          return "wlt_cheat: overlapping tiles in k = " + std::to_string(k);
+    s = e;
+  }
+  return "";
+}
+
 int spGEMM(csc CSC, csr CSR, wlt WLT, wlt_cheat WLT_C, int cheat) {
-  // The engine derives its own row workloads; the per-k tables (and the
-  // 2-D split pairs of the cheat table) are accepted for interface
-  // compatibility and not read.
-  (void)WLT;
-  (void)WLT_C;
-  (void)cheat;
   if (CSC.n != CSR.n) {
     LEGACY_FAIL(SPGEMM_ERR_INVALID, "spGEMM: A and B must both be n x n");
+    return -1;
+  }
+  if (!CSC.header || !CSR.header || CSC.n < 0) {
+    LEGACY_FAIL(SPGEMM_ERR_INVALID, "spGEMM: null pointer array");
+    return -1;
+  }
+  std::string bad = check_wlt(CSC, CSR, WLT);
+  if (bad.empty() && cheat) bad = check_wlt_cheat(CSC, CSR, WLT_C);
+  if (!bad.empty()) {
+    LEGACY_FAIL(SPGEMM_ERR_INVALID, ("spGEMM: " + bad).c_str());
     return -1;
   }
   CSC_HOST = CSC;

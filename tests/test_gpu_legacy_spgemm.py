@@ -126,3 +126,86 @@ def test_legacy_globals_and_state_errors():
     finally:
         L.spgemm_set_exit_on_error(1)
         L.spgemm_set_verbose(1)
+
+
+class WltData(C.Structure):
+    _fields_ = [("idx", C.c_int), ("base_idx", C.c_int), ("num_of_row_elements", C.c_int),
+                ("num_of_col_elements", C.c_int)]
+
+
+class Wlt(C.Structure):
+    _fields_ = [("data", C.POINTER(WltData)), ("threadblocks", C.c_int), ("workloads", C.c_int)]
+
+
+class WltDataCheat(C.Structure):
+    _fields_ = [("ridx", C.c_int), ("cidx", C.c_int), ("base_idx", C.c_int),
+                ("num_of_row_elements", C.c_int), ("num_of_col_elements", C.c_int)]
+
+
+class WltCheat(C.Structure):
+    _fields_ = [("data", C.POINTER(WltDataCheat)), ("threadblocks", C.c_int), ("workloads", C.c_int)]
+
+
+def test_spgemm_with_workload_tables():
+    """spGEMM() with a per-k table and a non-trivial 2-D tile table (heavy
+    outer products split into 7 x 5 tiles) gives the oracle's C; tables that
+    do not describe the operands are rejected with SPGEMM_ERR_INVALID."""
+    L = sg.lib()
+    L.spgemm_set_exit_on_error(0)
+    L.spgemm_set_verbose(0)
+    try:
+        A = W.rmat(11, 12, 8, values="sym")
+        B = W.rmat(11, 10, 9, values="sym")
+        a = A.to_csc()
+        keep = [np.ascontiguousarray(x) for x in (a.colptr, a.rowidx, a.val, B.rowptr, B.col, B.val)]
+        ip = lambda x: x.ctypes.data_as(C.POINTER(C.c_int))
+        fp = lambda x: x.ctypes.data_as(C.POINTER(C.c_float))
+        csc = CSC(ip(keep[0]), ip(keep[1]), fp(keep[2]), A.cols, A.nnz)
+        csr = CSR(ip(keep[3]), ip(keep[4]), fp(keep[5]), B.rows, B.nnz)
+        L.makeWLT.restype = Wlt
+        L.makeWLT.argtypes = [CSC, CSR]
+        L.makeWLT_cheat.restype = WltCheat
+        L.makeWLT_cheat.argtypes = [CSC, CSR, C.c_int, C.c_int, C.c_int]
+        L.spGEMM.restype = C.c_int
+        L.spGEMM.argtypes = [CSC, CSR, Wlt, WltCheat, C.c_int]
+        wl = L.makeWLT(csc, csr)
+        wc = L.makeWLT_cheat(csc, csr, 7, 5, 200)
+        assert wl.threadblocks > 0 and wc.threadblocks > 0
+        # at least one outer product is split into several tiles
+        tiles = [wc.data[t] for t in range(wc.threadblocks)]
+        assert any(t.num_of_col_elements == 7 or t.num_of_row_elements == 5 for t in tiles)
+        ref = oracle.spgemm(A.rows, B.cols, a.colptr, a.rowidx, a.val, B.rowptr, B.col, B.val,
+                            stats=True)
+        nnz = L.spGEMM(csc, csr, wl, wc, 1)
+        assert nnz == len(ref["col"])
+        n = A.rows
+        ptr = np.ctypeslib.as_array(C.POINTER(C.c_int).in_dll(L, "c_ptr_h"), (n + 1,)).copy()
+        col = np.ctypeslib.as_array(C.POINTER(C.c_int).in_dll(L, "c_idx_h"), (nnz,)).copy()
+        val = np.ctypeslib.as_array(C.POINTER(C.c_float).in_dll(L, "c_val_h"), (nnz,)).copy()
+        assert_structure_equal(ptr, col, ref["rowptr"], ref["col"])
+        assert_values_close(val, ref, plain_tolerance(ref))
+        # a tile that leaves its B row
+        t0 = wc.data[0]
+        saved = t0.num_of_row_elements
+        wc.data[0].num_of_row_elements = saved + 10 ** 6
+        assert L.spGEMM(csc, csr, wl, wc, 1) == -1
+        assert L.spgemm_legacy_status() == 1
+        # with cheat == 0 the tile table is not consulted
+        assert L.spGEMM(csc, csr, wl, wc, 0) == len(ref["col"])
+        wc.data[0].num_of_row_elements = saved
+        # a dropped tile leaves its outer product uncovered
+        short = WltCheat(wc.data, wc.threadblocks - 1, wc.workloads)
+        if wc.threadblocks > 1:
+            assert L.spGEMM(csc, csr, wl, short, 1) == -1
+        # a per-k record with the wrong element count
+        wl.data[0].num_of_col_elements += 1
+        assert L.spGEMM(csc, csr, wl, wc, 1) == -1
+        wl.data[0].num_of_col_elements -= 1
+        assert L.spGEMM(csc, csr, wl, wc, 1) == len(ref["col"])
+        L.freeWLT.argtypes = [C.POINTER(Wlt)]
+        L.freeWLTC.argtypes = [C.POINTER(WltCheat)]
+        L.freeWLT(C.byref(wl))
+        L.freeWLTC(C.byref(wc))
+    finally:
+        L.spgemm_set_exit_on_error(1)
+        L.spgemm_set_verbose(1)
