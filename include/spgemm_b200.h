@@ -90,6 +90,12 @@ typedef struct spgemm_tuning {
                              permitting) so the numeric pass skips rebuilding them */
     int mid_o_min;        /* long rows: span bitmap when nnz_i > this (else hash) */
     int mid_cols;         /* bitmap paths need a column span <= this (<= 2^18) */
+    int long_rows;        /* long rows in plain FP32 whose symbolic bitmaps were kept
+                             and whose column span is at most 2^18: 0 = column
+                             slices; 1 = one block per whole row, products reduced
+                             into C in L2; 2 = one block per whole row, shared-memory
+                             accumulation for rows of up to ~38K outputs (longer
+                             rows take column slices) */
 } spgemm_tuning;
 
 /* Library version string. */
@@ -226,22 +232,32 @@ int spgemm_read_mtx(coo* out, const char* path);
  * counterpart in the reference; it performs the conversion of cudaCOO2CM
  * (sorted triplets -> CSR for ROW_MAJOR, CSC for COL_MAJOR) on device arrays
  * the caller owns, for callers that cannot allocate device memory at that
- * point: work recorded into a CUDA graph, code whose device memory is owned by
- * another allocator, latency-critical loops in which a cudaMalloc would
- * synchronise the device.
- *   d_triplets: nnz triplets on the device, sorted by (major, minor) index;
+ * point: code whose device memory belongs to another allocator (a
+ * framework's caching allocator, a fixed arena sized up front), and
+ * latency-critical loops in which a cudaMalloc would synchronise the device.
+ *   d_triplets: nnz triplets on the device, sorted by (major, minor) index
+ *               with every index inside the dimensions;
  *   d_ptr: (major dimension + 1) ints; d_idx, d_val: nnz entries each.
  * Nothing is allocated: the counts are accumulated in d_ptr itself and the
  * scan's scratch is a fixed static device array of about 131 KB, present on
  * every GPU that loads this library until the process exits. It limits the
  * major dimension to SPGEMM_NOALLOC_MAX_MAJOR (larger: SPGEMM_ERR_TOO_LARGE,
- * nothing launched). The first call on a device looks up that array's device
- * address (and loads the kernels); make that first call before any stream
- * capture. All calls share the array: calls that can overlap on the GPU (on
- * different streams without ordering) race and must not be issued.
+ * nothing launched). The first call on a device, with that device current,
+ * looks up that array's device address and loads this entry point's kernels;
+ * make that first call before any stream capture. The address is kept per
+ * device ordinal for the process: only the runtime's primary context is
+ * supported, and the library must not be used on a device after
+ * cudaDeviceReset. All calls share the array, which keeps the previous
+ * call's contents (each call clears what must start at zero): calls that can
+ * overlap on the GPU (on different streams without ordering) race and must
+ * not be issued.
  * Asynchronous on `stream` unless nnz_check is non-null, in which case the
  * stream is synchronised, *nnz_check receives the number of entries counted,
- * and an out-of-range index or unsorted input returns SPGEMM_ERR_INVALID. */
+ * and an out-of-range index or unsorted input returns SPGEMM_ERR_INVALID.
+ * With nnz_check == NULL nothing is checked on the host: input that is
+ * unsorted or holds an out-of-range index gives undefined output (entries
+ * with an out-of-range index are skipped and leave their d_idx / d_val slots
+ * unwritten) while the call returns SPGEMM_OK. */
 #define SPGEMM_NOALLOC_MAX_MAJOR (1 << 26)
 int spgemm_coo_to_cm_noalloc(const triplet* d_triplets, int nnz, int num_rows,
                              int num_cols, int type, int* d_ptr, int* d_idx,

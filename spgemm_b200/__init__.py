@@ -61,7 +61,8 @@ class Tuning(C.Structure):
     _fields_ = [("warp_p_max", C.c_int), ("warp_table_max", C.c_int),
                 ("warp_cap_max", C.c_int), ("long_p", C.c_int), ("long_o_num", C.c_int),
                 ("slice_cap", C.c_int), ("slice_cols", C.c_int), ("sym_window", C.c_int),
-                ("keep_bitmaps", C.c_int), ("mid_o_min", C.c_int), ("mid_cols", C.c_int)]
+                ("keep_bitmaps", C.c_int), ("mid_o_min", C.c_int), ("mid_cols", C.c_int),
+                ("long_rows", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -47,6 +47,7 @@ Tuning default_tuning() {
   t.keep_bitmaps = 1;
   t.mid_o_min = 256;
   t.mid_cols = 1 << 18;
+  t.long_rows = 0;
   return t;
 }
 
@@ -112,7 +113,7 @@ Engine::~Engine() {
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
                    &chunk_cnt_, &slices_buf_, &mid_slices_, &row_span_, &counters_, &restrict_scratch_,
                    &tcap_, &toff_, &t_col_, &t_val_,
-                   &bitmaps_, &out_rowptr_,
+                   &bitmaps_, &lpt_order_, &out_rowptr_,
                    &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
   for (DevBuf& b : stage_) b.release();
@@ -149,6 +150,7 @@ int Engine::set_tuning(const Tuning& t) {
     return fail(1, "tuning: slice_cap must be 0 (auto) or >= 2048");
   if (t.mid_o_min < 0 || t.mid_cols < 0 || t.mid_cols > (1 << 18))
     return fail(1, "tuning: mid_o_min >= 0 and 0 <= mid_cols <= 2^18");
+  if (t.long_rows < 0 || t.long_rows > 2) return fail(1, "tuning: long_rows must be 0, 1 or 2");
   tn_ = t;
   return 0;
 }
@@ -388,7 +390,7 @@ int Engine::symbolic_pass(long long* nnz_c) {
         row_span_.as<int2>(), dc->num_count, num_rows_.as<int>(), chunk_cnt_.as<int>(),
         n_chunks_, long_slot_.as<int>(), slices_buf_.as<Slice>(), &dc->slice_count,
         (int)big_capacity_, mid_slices_.as<Slice>(), &dc->mid_count, bitmap_words_ > 0 ? 1 : 0,
-        &dc->status, tr);
+        &dc->status, tr, rows_cnt_max(), ROWS_MAX_WORDS);
     SG_LAUNCHED("k_num_bin");
   }
   if (replay_) {
@@ -610,6 +612,8 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   const long long* c_rowptr = c_rowptr64_.as<long long>();
   unsigned* status = &counters_.as<DevCounters>()->status;
   const int stride = 2 * max_row_len_ + 2;
+  if (MODE == 0 && rows_cnt_max() > 0)
+    if (int r = launch_num_rows(c_col, c_val)) return r;
   // big bitmap slices (long rows)
   if (nslices_ > 0) {
     const int dir_words = (int)(big_dir_bytes() / sizeof(uint2));
@@ -660,6 +664,68 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
 }
 
 template int Engine::launch_numeric_mode<0>(int*, float*);
+
+// Whole-row numeric path: reductions into C (long_rows = 1, any nnz_i) or
+// shared-memory accumulation (long_rows = 2, nnz_i up to the capacity that
+// one 1024-thread block's shared memory leaves after the directory). Plain
+// FP32 only, and only when the symbolic pass kept the long rows' bitmaps.
+static constexpr int ROWS_RED_THREADS = 512;
+static constexpr int ROWS_SMEM_THREADS = 1024;
+static constexpr size_t ROWS_SMEM_BUDGET = 225 * 1024;
+
+int Engine::rows_smem_cap() const {
+  const size_t fixed = (ROWS_SMEM_THREADS / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
+  return (int)((ROWS_SMEM_BUDGET - fixed) / sizeof(float));
+}
+
+int Engine::rows_cnt_max() const {
+  if (precision_ != 0 || tn_.long_rows == 0 || bitmap_words_ == 0 || n_long_sym_ == 0) return 0;
+  return tn_.long_rows == 1 ? 0x7fffffff : rows_smem_cap();
+}
+
+int Engine::launch_num_rows(int* c_col, float* c_val) {
+  DevCounters* dc = counters_.as<DevCounters>();
+  const int cnt = n_long_sym_;
+  const int* rows = sym_rows_.as<int>() + (size_t)FB_LONG * m_;
+  SG_CK(lpt_order_.ensure(sizeof(int) * (size_t)cnt), "alloc row order");
+  const int lb = blocks_for(cnt, 256, (long long)sms_ * 4);
+  const int cmax = rows_cnt_max();
+  prof_begin("k_lpt_hist");
+  k_lpt_hist<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+                                      row_span_.as<int2>(), cmax, ROWS_MAX_WORDS, dc->lpt_hist);
+  SG_LAUNCHED("k_lpt_hist");
+  prof_begin("k_lpt_scatter");
+  k_lpt_scatter<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+                                         row_span_.as<int2>(), cmax, ROWS_MAX_WORDS, dc->lpt_hist,
+                                         dc->lpt_cursor, lpt_order_.as<int>(), &dc->rows_listed);
+  SG_LAUNCHED("k_lpt_scatter");
+  const Operands op = op_;
+  unsigned* status = &dc->status;
+  if (tn_.long_rows == 1) {
+    constexpr int NT = ROWS_RED_THREADS;
+    const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
+    SG_CK(smem_attr(k_num_rows<NT, true>, smem), "smem attr k_num_rows");
+    prof_begin("k_num_rows");
+    k_num_rows<NT, true><<<blocks_for(cnt, 1, (long long)sms_ * 2), NT, smem, stream_>>>(
+        op, lpt_order_.as<int>(), &dc->rows_listed, &dc->row_queue, row_p_.as<long long>(),
+        c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
+        long_slot_.as<int>(), ROWS_MAX_WORDS, 0, c_col, c_val, status);
+    SG_LAUNCHED("k_num_rows");
+  } else {
+    constexpr int NT = ROWS_SMEM_THREADS;
+    const int cap = rows_smem_cap();
+    const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
+                        (size_t)cap * sizeof(float);
+    SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
+    prof_begin("k_num_rows");
+    k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_), NT, smem, stream_>>>(
+        op, lpt_order_.as<int>(), &dc->rows_listed, &dc->row_queue, row_p_.as<long long>(),
+        c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
+        long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
+    SG_LAUNCHED("k_num_rows");
+  }
+  return 0;
+}
 template int Engine::launch_numeric_mode<1>(int*, float*);
 
 int Engine::multiply(const cm& A, const cm& B, cm* C_dev) {

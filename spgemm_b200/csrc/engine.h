@@ -35,6 +35,10 @@ struct DevCounters {
   long long grand_total;
   int max_row_len;  // longest row of A (entries)
   int overflow_count;  // warp-bin rows redone by the mid / block kernels
+  int lpt_hist[32];    // whole-row numeric path: rows per work group,
+  int lpt_cursor[32];  // fill cursors of the work order,
+  int rows_listed;     // rows in the work order,
+  int row_queue;       // and the dynamic row queue
 };
 
 class Engine {
@@ -131,6 +135,12 @@ class Engine {
   int launch_numeric_bins(int* c_col, float* c_val);
   template <int MODE> int launch_numeric_mode(int* c_col, float* c_val);
   size_t big_dir_bytes() const;
+  // Whole-row numeric path of the long rows (k_num_rows): the largest nnz_i
+  // it takes for this product (0: path off), its shared-memory value
+  // capacity, and its launch.
+  int rows_cnt_max() const;
+  int rows_smem_cap() const;
+  int launch_num_rows(int* c_col, float* c_val);
   int scan_counts(const int* in, int n, long long* out);
   int check_status(unsigned st);
   template <class K> cudaError_t smem_attr(K kernel, size_t bytes);
@@ -167,7 +177,7 @@ class Engine {
   DevBuf row_p_, c_cnt_, c_rowptr64_, tiles_;
   DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_, mid_slices_, row_span_;
   DevBuf tcap_, toff_, t_col_, t_val_;  // fused pass: row bounds, temp offsets, temp output
-  DevBuf counters_, restrict_scratch_, bitmaps_;
+  DevBuf counters_, restrict_scratch_, bitmaps_, lpt_order_;
   int bitmap_words_ = 0;  // per long row; 0 when the bitmaps are not kept
   int max_row_len_ = 0;
   DevBuf out_rowptr_, out_col_, out_val_;

@@ -82,7 +82,20 @@ struct Tuning {
   int keep_bitmaps;     // keep long rows' symbolic bitmaps for the numeric pass
   int mid_o_min;        // long rows: bitmap numeric when nnz_i > this ...
   int mid_cols;         // bitmap paths need a column span of at most this (<= 2^18)
+  int long_rows;        // long rows, plain FP32, bitmaps kept: 0 column slices;
+                        // 1 whole rows, reductions into C (L2); 2 whole rows,
+                        // shared-memory accumulation (rows up to its capacity)
 };
+
+// Whole-row numeric path (k_num_rows): the row's column span must fit the
+// block's directory, and (shared-memory form) its outputs the value array.
+constexpr int ROWS_MAX_WORDS = (1 << 18) / 32 + 1;  // 2^18 columns, + lo rounded down
+
+__host__ __device__ inline bool whole_row_path(int o, int2 sp, int cnt_max, int max_words) {
+  if (o <= 0 || o > cnt_max) return false;
+  const int lo = sp.x & ~31;
+  return ((sp.y + 1 - lo + 31) >> 5) <= max_words;
+}
 
 __host__ __device__ inline int ceil_log2_ll(long long v) {
   int r = 0;

@@ -1,18 +1,20 @@
 // Allocation-free COO -> CSR/CSC conversion (spgemm_coo_to_cm_noalloc).
 //
 // Some callers cannot call cudaMalloc at the point where they convert a
-// matrix: code recorded into a CUDA graph, code running under an allocator
-// that owns all device memory (a framework's caching allocator, a fixed
-// arena), or latency-sensitive loops where an allocation would synchronise the
-// device. They still own the input triplets and the output arrays, so this
-// entry point only needs scratch for its prefix scan; that scratch lives in a
+// matrix: code running under an allocator that owns all device memory (a
+// framework's caching allocator, a fixed arena sized up front), or
+// latency-sensitive loops where an allocation would synchronise the device.
+// They still own the input triplets and the output arrays, so this entry
+// point only needs scratch for its prefix scan; that scratch lives in a
 // file-scope __device__ array instead of being allocated.
 //
 // The array is fixed in size (SPGEMM_NOALLOC_MAX_MAJOR rows or columns at
 // most) and exists on every GPU that loads this library until the process
 // exits. Host code must not pass the array's name to a kernel (in host code
 // it is only a stand-in symbol); the device address is looked up once per
-// device with cudaGetSymbolAddress, on the first call made on that device.
+// device with cudaGetSymbolAddress, on the first call made on that device,
+// which also loads this file's kernels (so that no later call is the first
+// use of a kernel under lazy module loading).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -152,7 +154,8 @@ na_apply(int* __restrict__ ptr, int n, const long long* __restrict__ scratch) {
 }
 
 // Device address of g_noalloc_scratch on the current device (looked up on
-// the first call made on that device).
+// the first call made on that device, which also loads the kernels: a
+// cudaFuncGetAttributes query loads a kernel's module without launching it).
 cudaError_t scratch_for_current_device(long long** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -160,6 +163,15 @@ cudaError_t scratch_for_current_device(long long** out) {
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_setup_mutex);
   if (!g_scratch_dev[dev]) {
+    cudaFuncAttributes fa;
+    const void* kernels[] = {reinterpret_cast<const void*>(na_split),
+                             reinterpret_cast<const void*>(na_tile_sums),
+                             reinterpret_cast<const void*>(na_tile_offsets),
+                             reinterpret_cast<const void*>(na_apply)};
+    for (const void* k : kernels) {
+      e = cudaFuncGetAttributes(&fa, k);
+      if (e != cudaSuccess) return e;
+    }
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;

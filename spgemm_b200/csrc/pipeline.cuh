@@ -816,14 +816,17 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
           const int* __restrict__ chunk_cnt, int n_chunks, const int* __restrict__ long_slot,
           Slice* __restrict__ big, int* __restrict__ big_count, int big_capacity,
           Slice* __restrict__ mid, int* __restrict__ mid_count, int bits_kept,
-          unsigned* status, Tuning tn) {
+          unsigned* status, Tuning tn, int rows_cnt_max, int rows_max_words) {
   __shared__ int hist[NB_COUNT], base[NB_COUNT];
   const int i = blockIdx.x * NBIN_THREADS + threadIdx.x;
   if (threadIdx.x < NB_COUNT) hist[threadIdx.x] = 0;
   __syncthreads();
   int bin = -1, rank = 0;
   bool listed = false;  // bitmap rows go to a slice list, not a row list
-  if (i < m && row_p[i] > tn.long_p) {  // other rows were done by the fused pass
+  // other rows were done by the fused pass; rows_cnt_max > 0: rows that the
+  // whole-row kernel takes are left to it
+  if (i < m && row_p[i] > tn.long_p &&
+      !(rows_cnt_max > 0 && whole_row_path(c_cnt[i], row_span[i], rows_cnt_max, rows_max_words))) {
     const int o = c_cnt[i];
     const long long p = row_p[i];
     bin = num_bin_of(o, p, tn);
@@ -1168,6 +1171,178 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       // leave the directory clean for the next slice
       for (int t = threadIdx.x; t < nt; t += NT) dir[touched[t]] = make_uint2(0u, 0u);
       for (int t = threadIdx.x; t < l1_words; t += NT) l1[t] = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Numeric pass: whole long rows, one block per row (plain FP32)
+// ---------------------------------------------------------------------------
+
+// Work order of the long rows: grouped by floor(log2 P_i), heaviest group
+// first, so that on the dynamic row queue of k_num_rows the longest rows
+// start first and the short ones fill in at the end (longest-processing-time
+// first, to a factor of two). Only the rows whole_row_path() accepts are listed.
+constexpr int LPT_GROUPS = 32;
+
+__device__ __forceinline__ int lpt_group(long long p) { return 63 - __clzll(p > 0 ? p : 1); }
+
+__global__ void __launch_bounds__(256)
+k_lpt_hist(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
+           const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_max,
+           int max_words, int* __restrict__ hist) {
+  __shared__ int h[LPT_GROUPS];
+  if (threadIdx.x < LPT_GROUPS) h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
+    const int i = rows[r];
+    if (whole_row_path(c_cnt[i], row_span[i], cnt_max, max_words))
+      atomicAdd(&h[min(lpt_group(row_p[i]), LPT_GROUPS - 1)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < LPT_GROUPS && h[threadIdx.x]) atomicAdd(hist + threadIdx.x, h[threadIdx.x]);
+}
+
+// hist: rows per group (from k_lpt_hist); cursor: zeroed per group counters;
+// order: the listed rows, heaviest group first; *nlisted: their count.
+__global__ void __launch_bounds__(256)
+k_lpt_scatter(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
+              const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_max,
+              int max_words, const int* __restrict__ hist, int* __restrict__ cursor,
+              int* __restrict__ order, int* __restrict__ nlisted) {
+  __shared__ int base[LPT_GROUPS];
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int g = LPT_GROUPS - 1; g >= 0; --g) {
+      base[g] = run;
+      run += hist[g];
+    }
+    if (blockIdx.x == 0) *nlisted = run;
+  }
+  __syncthreads();
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
+    const int i = rows[r];
+    if (whole_row_path(c_cnt[i], row_span[i], cnt_max, max_words)) {
+      const int g = min(lpt_group(row_p[i]), LPT_GROUPS - 1);
+      order[base[g] + atomicAdd(cursor + g, 1)] = i;
+    }
+  }
+}
+
+// Value functors of k_num_rows: the product lands in the output slot given by
+// its column's rank in the row's directory, either as a reduction into C in
+// global memory (performed in L2; nothing is returned to the SM) or as a
+// shared-memory atomic add.
+__device__ __forceinline__ void red_add_f32(float* p, float v) {
+  asm volatile("red.global.add.f32 [%0], %1;" ::"l"(p), "f"(v) : "memory");
+}
+
+struct RowValRed {
+  const uint2* dir;
+  float* out;  // C values of the row
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if ((unsigned)(col - lo) < width) red_add_f32(out + long_slot(dir, lo, col), __fmul_rn(a, b));
+  }
+};
+
+struct RowValSmem {
+  const uint2* dir;
+  float* vals;  // shared memory, one slot per output
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if ((unsigned)(col - lo) < width) atomicAdd(vals + long_slot(dir, lo, col), __fmul_rn(a, b));
+  }
+};
+
+// One block per long row, rows taken from a queue in LPT order. The row's
+// presence bitmap, kept by the symbolic pass, is loaded for the whole column
+// span into a shared-memory directory (bits + rank of the first column of
+// every 32-column word); every product then adds into its final position
+// out0 + rank(column), so the row is produced in column order with no
+// column slicing and no sort. RED: values accumulate in C itself (zeroed
+// first; the row's value range stays in L2 while the block works on it);
+// otherwise in shared memory (rows of at most `cap` outputs), copied out at
+// the end. Columns are written from the directory. Shared memory: per-warp
+// scratch | directory uint2[dir_words] | (not RED) values float[cap].
+template <int NT, bool RED>
+__global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 2)
+k_num_rows(Operands op, const int* __restrict__ order, const int* __restrict__ nrows_p,
+           int* __restrict__ queue, const long long* __restrict__ row_p,
+           const long long* __restrict__ c_rowptr, const int2* __restrict__ row_span,
+           const unsigned* __restrict__ bitmaps, int bitmap_words,
+           const int* __restrict__ long_slot_of, int dir_words, int cap,
+           int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
+  constexpr int NW = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ long long scan_shm[33];
+  __shared__ int s_item;
+  const int warp = threadIdx.x >> 5;
+  SegScratch* sc = reinterpret_cast<SegScratch*>(smem) + warp;
+  uint2* dir = reinterpret_cast<uint2*>(smem + NW * sizeof(SegScratch));
+  float* vals = reinterpret_cast<float*>(dir + dir_words);
+  const int nrows = *nrows_p;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(queue, 1);
+    __syncthreads();
+    const int r = s_item;
+    if (r >= nrows) break;
+    const int i = order[r];
+    const long long out0 = c_rowptr[i];
+    const int cnt = (int)(c_rowptr[i + 1] - out0);
+    const int2 sp = row_span[i];
+    const int lo = sp.x & ~31;  // word aligned: the kept bitmaps are indexed from column 0
+    const int nw = (sp.y + 1 - lo + 31) >> 5;
+    if (nw > dir_words || (!RED && cnt > cap)) {  // the host's sizing prevents this
+      if (threadIdx.x == 0) atomicOr(status, ST_SLICE_OVERFLOW);
+      __syncthreads();
+      continue;
+    }
+    const unsigned* src = bitmaps + (size_t)long_slot_of[i] * bitmap_words + (lo >> 5);
+    for (int t = threadIdx.x; t < nw; t += NT) dir[t] = make_uint2(__ldg(src + t), 0u);
+    __syncthreads();
+    const long long tot = dir_ranks<NT>(dir, nw, [](int t) { return t; }, scan_shm);
+    if (tot != cnt) {  // block-uniform
+      if (threadIdx.x == 0) atomicOr(status, ST_COUNT_MISMATCH);
+      __syncthreads();
+      continue;
+    }
+    if (RED) {
+      for (int t = threadIdx.x; t < cnt; t += NT) c_val[out0 + t] = 0.f;
+    } else {
+      for (int t = threadIdx.x; t < cnt; t += NT) vals[t] = 0.f;
+    }
+    __syncthreads();  // ranks and zeroed values visible to the whole block
+    const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
+    const int p = (int)row_p[i];
+    const int U = chunk_for(p, NW, 1 << 20);
+    const unsigned width = (unsigned)(sp.y + 1 - lo);
+    if (RED) {
+      RowValRed f{dir, c_val + out0, lo, width};
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+    } else {
+      RowValSmem f{dir, vals, lo, width};
+      for (int c0 = warp * U; c0 < p; c0 += NW * U)
+        warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+    }
+    __syncthreads();
+    // columns (and shared-memory values) in rank order, one directory word
+    // per thread at a time
+    for (int w = threadIdx.x; w < nw; w += NT) {
+      const uint2 d = dir[w];
+      unsigned b = d.x;
+      int pos = (int)d.y;
+      while (b) {
+        const int bit = __ffs(b) - 1;
+        b &= b - 1u;
+        __stcs(c_col + out0 + pos, lo + 32 * w + bit);
+        if (!RED) __stcs(c_val + out0 + pos, vals[pos]);
+        ++pos;
+      }
     }
     __syncthreads();
   }

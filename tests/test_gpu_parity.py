@@ -163,6 +163,10 @@ TUNINGS = [
     dict(sym_window=4096, slice_cols=4096, slice_cap=2048,  # multi-window symbolic pass,
          keep_bitmaps=0),                                   # restricted numeric slices
     dict(mid_cols=0),                                       # no bitmaps: hash tables only
+    dict(long_rows=1),                                      # whole long rows, reductions into C
+    dict(long_rows=2),                                      # whole long rows, shared memory
+    dict(long_rows=1, long_p=256, long_o_num=256),          # ... with many short long rows
+    dict(long_rows=2, keep_bitmaps=0),                      # no kept bitmaps: column slices
 ]
 
 
@@ -182,6 +186,40 @@ def test_tuning_overrides(tuning, precision):
         assert stats["long_row_slices"] > stats["rows_per_numeric_bin"][8], stats
 
 
+@pytest.mark.parametrize("long_rows", [1, 2])
+def test_whole_row_path_with_wide_and_narrow_rows(long_rows):
+    """Long rows of both kinds in one product: row 0 has ~90K outputs (beyond
+    the shared-memory capacity of long_rows=2, so it takes column slices
+    there), rows 1..3 a few thousand; n = 200K keeps every span inside the
+    whole-row directory."""
+    rng = np.random.default_rng(21)
+    n, kk = 200_000, 300
+    rows, cols = [], []
+    for k in range(kk):
+        c = np.unique(rng.integers(0, n, 400))
+        rows.append(np.full(len(c), k))
+        cols.append(c)
+    rows.append(np.full(2, kk)); cols.append(np.array([7, 8]))
+    r = np.concatenate(rows)
+    c = np.concatenate(cols)
+    B = W.from_coo(kk + 1, n, r, c, rng.uniform(-1, 1, len(r)).astype(np.float32))
+    ar = np.array([0] * kk + [1] * 20 + [2] * 25 + [3] * 30)
+    ac = np.array(list(range(kk)) + list(range(20)) + list(range(100, 125)) + list(range(200, 230)))
+    A = W.from_coo(4, kk + 1, ar, ac, rng.uniform(-1, 1, len(ar)).astype(np.float32))
+    with sg.Handle() as h:
+        h.set_tuning(long_rows=long_rows)
+        C = h.multiply_host(A.to_csc(), B)
+        stats = h.stats()
+    ref = ref_product(A, B)
+    assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+    assert_values_close(C.val, ref, plain_tolerance(ref))
+    assert np.diff(ref["rowptr"])[0] > 40_000
+    if long_rows == 2:
+        assert stats["long_row_slices"] >= 2, stats  # row 0 was sliced
+    else:
+        assert stats["long_row_slices"] == 0, stats
+
+
 def test_bad_tuning_rejected():
     with sg.Handle() as h:
         with pytest.raises(sg.SpgemmError):
@@ -192,6 +230,8 @@ def test_bad_tuning_rejected():
             h.set_tuning(long_p=5000)
         with pytest.raises(sg.SpgemmError):
             h.set_tuning(warp_table_max=100)
+        with pytest.raises(sg.SpgemmError):
+            h.set_tuning(long_rows=3)
 
 
 def _dev(a, dtype, offset=0):

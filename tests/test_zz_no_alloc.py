@@ -1,9 +1,11 @@
 """spgemm_coo_to_cm_noalloc: the allocation-free conversion for callers that
-cannot allocate device memory (graph capture, foreign allocators, hot loops).
-Called through the C ABI on caller-owned device arrays, its output must equal
-cudaCOO2CM's (the same conversion, which allocates its own workspace) on two
-calls in a row that share the static scratch array. This file sorts last so
-that a run stopping at the first failure has run every other test."""
+cannot allocate device memory (device memory owned by another allocator, hot
+loops where a cudaMalloc would synchronise). Called through the C ABI on
+caller-owned device arrays, its output must equal cudaCOO2CM's (the same
+conversion, which allocates its own workspace) and the CSR/CSC the triplets
+were made from, on two calls in a row that share the static scratch array.
+This file sorts last so that a run stopping at the first failure has run
+every other test."""
 import ctypes as C
 
 import numpy as np
@@ -76,6 +78,38 @@ def test_noalloc_matches_cudaCOO2CM_twice():
         got = noalloc_conversion(t, M.rows, M.cols, kind)
         for a, b in zip(ref, got):
             assert np.array_equal(a, b)
+        # and the compressed matrix the triplets were made from
+        src = M if kind == sg.ROW_MAJOR else M.to_csc()
+        ptr, idx, val = ((src.rowptr, src.col, src.val) if kind == sg.ROW_MAJOR
+                         else (src.colptr, src.rowidx, src.val))
+        assert np.array_equal(got[0], ptr)
+        assert np.array_equal(got[1], idx)
+        assert np.array_equal(got[2], val)
+
+
+def test_noalloc_empty_input():
+    import torch
+    d_ptr = torch.full((6,), -7, dtype=torch.int32, device="cuda")
+    total = C.c_longlong(-1)
+    st = lib().spgemm_coo_to_cm_noalloc(None, 0, 5, 9, sg.ROW_MAJOR, d_ptr.data_ptr(), None,
+                                        None, None, C.byref(total))
+    assert st == 0 and total.value == 0
+    assert np.array_equal(d_ptr.cpu().numpy(), np.zeros(6, np.int32))
+
+
+def test_noalloc_reports_out_of_range_index():
+    import torch
+    # row index 3 == num_rows: out of range
+    t = np.array([[0, 1, 0], [1, 0, 0], [3, 2, 0]], np.int32)
+    d_t = torch.from_numpy(t).cuda()
+    bufs = [torch.zeros(4, dtype=torch.int32, device="cuda"),
+            torch.zeros(3, dtype=torch.int32, device="cuda"),
+            torch.zeros(3, dtype=torch.float32, device="cuda")]
+    total = C.c_longlong()
+    st = lib().spgemm_coo_to_cm_noalloc(d_t.data_ptr(), 3, 3, 3, sg.ROW_MAJOR, bufs[0].data_ptr(),
+                                        bufs[1].data_ptr(), bufs[2].data_ptr(), None, C.byref(total))
+    assert st == 1
+    assert total.value == 2  # the two entries inside the dimensions were counted
 
 
 def test_noalloc_rejects_oversize_and_reports_unsorted():
