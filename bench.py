@@ -63,12 +63,25 @@ def parse_args():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=8.0)
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the per-configuration suite of the default line")
+    p.add_argument("--tune", default="",
+                   help="tuning overrides for the GPU arm, e.g. long_rows=1,long_p=2048")
     return p.parse_args()
 
 
 # ---------------------------------------------------------------------------
 # workloads
 # ---------------------------------------------------------------------------
+
+def tune_overrides(args):
+    """--tune "k=v,k=v" as a dict of spgemm_tuning fields."""
+    out = {}
+    for kv in filter(None, args.tune.split(",")):
+        k, v = kv.split("=")
+        out[k.strip()] = int(v)
+    return out
+
 
 def build_workload(args):
     from spgemm_b200 import workloads as W
@@ -126,6 +139,10 @@ def product_stats(A, B):
 # Mirrors of the engine's default bin rules (kernels.cuh), used only to
 # attribute algorithmic bytes to the kernel that processed each row.
 LONG_P, WARP_CAP, WARP_TMAX, MID_COLS, LONG_O, MID_O = 4096, 2048, 256, 1 << 18, 4096, 256
+# output capacities of the whole-row kernel's two block sizes (engine.cu:
+# (shared-memory budget - per-warp scratch - directory) / 4 bytes)
+ROWS_CAP_512 = (111 * 1024 - 16 * 388 - 8193 * 8) // 4
+ROWS_CAP_1024 = (225 * 1024 - 32 * 388 - 8193 * 8) // 4
 
 
 def first_bin(p, cap, span):
@@ -145,8 +162,15 @@ def kernel_rows(name, p_i, o_i, span, n):
     long_rows = p_i > LONG_P
     if name == "k_sym_long":
         return long_rows, False
+    # whole long rows (default long_rows=2): up to ROWS_CAP_512 outputs in
+    # 512-thread blocks, up to ROWS_CAP_1024 in 1024-thread blocks, column
+    # slices (k_num_long) above
+    if name == "k_num_rows<512>":
+        return long_rows & (o_i > 0) & (o_i <= ROWS_CAP_512) & (span <= (1 << 18)), True
+    if name == "k_num_rows<1024>":
+        return long_rows & (o_i > ROWS_CAP_512) & (o_i <= ROWS_CAP_1024) & (span <= (1 << 18)), True
     if name == "k_num_long":
-        return long_rows & (o_i > LONG_O), True
+        return long_rows & (o_i > LONG_O) & ((o_i > ROWS_CAP_1024) | (span > (1 << 18))), True
     if name == "k_num_mid":
         return long_rows & (o_i > MID_O) & (o_i <= LONG_O) & (span <= MID_COLS), True
     if name == "k_fused_mid":
@@ -355,27 +379,17 @@ def batch_products(pairs):
     return P, ab
 
 
-def run_batch(args):
-    """Batched form: every step recomputes all products from the operands in
-    HBM by one replay of the batch's CUDA graph (pack, analysis, fused and
-    long-row passes of the packed block-diagonal product, per-product row
-    pointers), tuned by spgemm_b200.autotune. Compared with the plain path:
-    the same products one spgemm_multiply call each."""
-    specs, pairs = build_batch(args.batch_count)  # before any CUDA use (spawned workers)
+def measure_batch(args, dev, stream, pairs, steps, warmup, loop_steps, rank=0, dist=None,
+                  smi_id="0"):
+    """The batched form's measurement: operands uploaded into one device
+    arena per array kind, the batch planned (autotuned unless --no-autotune),
+    `steps` graph replays timed with CUDA events (L2 flushed before each),
+    the kernel split of one step, and the plain loop (one spgemm_multiply per
+    product) timed `loop_steps` times. Returns a dict; its handle "hb" stays
+    open for the caller."""
     import torch
     import spgemm_b200 as sg
     from spgemm_b200 import autotune
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(local)
-    dev = torch.device("cuda", local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    stream = torch.cuda.current_stream()
     P, alg_in = batch_products(pairs)
 
     # operands in one device arena per array kind (inputs stay resident)
@@ -407,6 +421,8 @@ def run_batch(args):
     torch.cuda.synchronize()
 
     hb = sg.Handle(sg.PLAIN)
+    if tune_overrides(args):
+        hb.set_tuning(**tune_overrides(args))
     hb.set_stream(stream.cuda_stream)
     if args.no_autotune:
         nnz_total = hb.batch_plan(A_list, B_list)
@@ -415,20 +431,18 @@ def run_batch(args):
         tune = autotune.tune_batch(hb, A_list, B_list, torch.cuda.get_device_name(dev), cache=None)
         nnz_total = hb.stats()["nnz_c"]
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
-    for _ in range(max(args.warmup, 0)):
+    for _ in range(max(warmup, 0)):
         hb.batch_execute(graph=True)
     torch.cuda.synchronize()
     launches0 = hb.stats()["kernel_launches"]
     if dist:
         dist.barrier()
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
-    smi_id = vis.split(",")[local].strip() if vis else str(local)
     sampler = ClockSampler(smi_id) if rank == 0 else None
     if sampler:
         sampler.start()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    for k in range(args.steps):
+          for _ in range(steps)]
+    for k in range(steps):
         flush.zero_()
         ev[k][0].record(stream)
         hb.batch_execute(graph=True)
@@ -442,7 +456,6 @@ def run_batch(args):
         t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = 2.0 * P * args.steps * world / (total_ms / 1e3) / 1e9
 
     # kernel split of one step (direct launches with timing events; untimed)
     hb.reset_kernel_times()
@@ -458,7 +471,7 @@ def run_batch(args):
         hp.multiply(A_cm, B_cm)
     torch.cuda.synchronize()
     loop_ms = []
-    for _ in range(max(args.loop_steps, 1)):
+    for _ in range(max(loop_steps, 1)):
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         flush.zero_()
         s0.record(stream)
@@ -469,6 +482,43 @@ def run_batch(args):
         loop_ms.append(s0.elapsed_time(s1))
     loop_step = float(np.median(loop_ms))
     hp.close()
+    del flush
+    ro, no = hb.batch_offsets()
+    return {"hb": hb, "P": P, "alg_in": alg_in, "kinds": kinds, "nnz_total": nnz_total,
+            "tune": tune, "step_ms": step_ms, "total_ms": total_ms, "clocks": clocks,
+            "launches": launches, "ktimes": ktimes, "loop_step": loop_step, "ro": ro, "no": no}
+
+
+def run_batch(args):
+    """Batched form: every step recomputes all products from the operands in
+    HBM by one replay of the batch's CUDA graph (pack, analysis, fused and
+    long-row passes of the packed block-diagonal product, per-product row
+    pointers), tuned by spgemm_b200.autotune. Compared with the plain path:
+    the same products one spgemm_multiply call each."""
+    specs, pairs = build_batch(args.batch_count)  # before any CUDA use (spawned workers)
+    import torch
+    import spgemm_b200 as sg
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    stream = torch.cuda.current_stream()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    smi_id = vis.split(",")[local].strip() if vis else str(local)
+    res = measure_batch(args, dev, stream, pairs, args.steps, args.warmup, args.loop_steps,
+                        rank, dist, smi_id)
+    hb, P, alg_in, kinds = res["hb"], res["P"], res["alg_in"], res["kinds"]
+    nnz_total, tune, step_ms, total_ms = res["nnz_total"], res["tune"], res["step_ms"], res["total_ms"]
+    clocks, launches, ktimes, loop_step = res["clocks"], res["launches"], res["ktimes"], res["loop_step"]
+    ro = res["ro"]
+    value = 2.0 * P * args.steps * world / (total_ms / 1e3) / 1e9
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     # e2e: operand arrays host->device (pinned), the batch, all of C device->host
     ro, no = hb.batch_offsets()
@@ -551,6 +601,307 @@ def run_batch(args):
 
 
 # ---------------------------------------------------------------------------
+# configuration suite: every configuration of the benchmark, one line
+# ---------------------------------------------------------------------------
+
+def _csr64(M, absval=False):
+    import warnings
+    import torch
+    warnings.filterwarnings("ignore", message="Sparse")
+    v = np.asarray(M.val, np.float64)
+    return torch.sparse_csr_tensor(
+        torch.from_numpy(np.asarray(M.rowptr, np.int64)),
+        torch.from_numpy(np.asarray(M.col, np.int64)),
+        torch.from_numpy(np.abs(v) if absval else v), size=(M.rows, M.cols)).cuda()
+
+
+def _sorted_entries(C, rows, ncols):
+    import torch
+    crow, col, val = C.crow_indices(), C.col_indices(), C.values()
+    r = torch.repeat_interleave(torch.arange(rows, device=col.device), crow.diff())
+    key = r * ncols + col
+    order = torch.argsort(key)
+    return key[order], val[order]
+
+
+def fp64_product(A, B):
+    """C = A*B in FP64 on the GPU by torch's sparse CSR product (cuSPARSE): an
+    independent checker for the error report, not the engine. Returns the
+    sorted keys (row * n + col) of C's entries, their FP64 values, and the
+    keys and values of |A|*|B| (sum of |p| per entry)."""
+    k, v = _sorted_entries(_csr64(A) @ _csr64(B), A.rows, B.cols)
+    ka, va = _sorted_entries(_csr64(A, True) @ _csr64(B, True), A.rows, B.cols)
+    return k, v, ka, va
+
+
+def fp64_chain(Pt, A, Pm):
+    """P^T (A P) in FP64 on the GPU (torch / cuSPARSE), as fp64_product."""
+    k, v = _sorted_entries(_csr64(Pt) @ (_csr64(A) @ _csr64(Pm)), Pt.rows, Pm.cols)
+    ka, va = _sorted_entries(_csr64(Pt, True) @ (_csr64(A, True) @ _csr64(Pm, True)), Pt.rows,
+                             Pm.cols)
+    return k, v, ka, va
+
+
+def rel_error_vs(ref, key, val):
+    """Errors of the engine's entries (key, val) against an FP64 product
+    `ref` = (keys, values, |p|-sum keys, |p|-sum values): max |v - c| / |c|
+    over entries with c != 0, the condition sum|p| / |c| of that entry, and
+    max |v - c| / sum|p| (the quantity the FP32 summation bound
+    gamma_n * sum|p| limits). Entries the FP64 product does not store count
+    as c = 0."""
+    import torch
+    k64, v64, ka, va = ref
+
+    def at(keys, vals):
+        if keys.numel() == 0:
+            return torch.zeros_like(val, dtype=torch.float64)
+        pos = torch.searchsorted(keys, key).clamp(max=keys.numel() - 1)
+        return torch.where(keys[pos] == key, vals[pos], torch.zeros_like(vals[pos]))
+    c, absum = at(k64, v64), at(ka, va)
+    err = (val.double() - c).abs()
+    nz = c != 0
+    out = {"zero_entries": int((~nz).sum())}
+    if bool(nz.any()):
+        rel = torch.where(nz, err / c.abs().clamp(min=1e-300), torch.zeros_like(err))
+        w = int(torch.argmax(rel))
+        out.update(max_rel=float(rel[w]), worst_cond=float(absum[w] / c[w].abs()))
+    else:
+        out.update(max_rel=0.0, worst_cond=0.0)
+    pos = absum > 0
+    out["max_err_over_abssum"] = float((err[pos] / absum[pos]).max()) if bool(pos.any()) else 0.0
+    return out
+
+
+def sampled_row_error(A, B, rp, col, val, nrows=2048, heavy=32):
+    """Relative error of C's rows for a sample (nrows random rows and the
+    `heavy` rows with the most products) against the FP64 product of those
+    rows of A with B (fp64_product)."""
+    import torch
+    from spgemm_b200 import workloads as W
+    p_i = product_stats(A, B)[0]
+    rng = np.random.default_rng(0)
+    rows = np.unique(np.concatenate([rng.choice(A.rows, min(nrows, A.rows), replace=False),
+                                     np.argsort(p_i)[-heavy:]])).astype(np.int64)
+    arp = A.rowptr.astype(np.int64)
+    lens = arp[rows + 1] - arp[rows]
+    sel = np.concatenate([np.arange(arp[i], arp[i + 1]) for i in rows])
+    Asub = W.Csr(len(rows), A.cols, np.concatenate([[0], np.cumsum(lens)]).astype(np.int32),
+                 A.col[sel], A.val[sel])
+    ref = fp64_product(Asub, B)
+    rp_h = rp.cpu().numpy().astype(np.int64)
+    clen = rp_h[rows + 1] - rp_h[rows]
+    pos = torch.from_numpy(np.concatenate([np.arange(rp_h[i], rp_h[i + 1]) for i in rows])).cuda()
+    sub_row = torch.from_numpy(np.repeat(np.arange(len(rows), dtype=np.int64), clen)).cuda()
+    key = sub_row * B.cols + col[pos].long()
+    err = rel_error_vs(ref, key, val[pos])
+    err["rows_checked"] = int(len(rows))
+    return err
+
+
+def engine_keys(rp, col, n):
+    import torch
+    rows = torch.repeat_interleave(torch.arange(rp.numel() - 1, device=col.device),
+                                   rp.long().diff())
+    return rows * n + col.long()
+
+
+class DeviceProduct:
+    """One product through the C ABI on device-resident operands (A as CSC,
+    B as CSR), output into preallocated device arrays."""
+
+    def __init__(self, sg, torch, dev, stream, A, B, precision, tune):
+        up = lambda a, t: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype=t)
+        Ac = A.to_csc()
+        self.keep = [up(Ac.colptr, torch.int32), up(Ac.rowidx, torch.int32), up(Ac.val, torch.float32),
+                     up(B.rowptr, torch.int32), up(B.col, torch.int32), up(B.val, torch.float32)]
+        k = self.keep
+        self.A = sg.device_cm(k[0].data_ptr(), k[1].data_ptr(), k[2].data_ptr(), A.nnz, A.rows,
+                              A.cols, sg.COL_MAJOR)
+        self.B = sg.device_cm(k[3].data_ptr(), k[4].data_ptr(), k[5].data_ptr(), B.nnz, B.rows,
+                              B.cols, sg.ROW_MAJOR)
+        self.h = sg.Handle(precision)
+        if tune:
+            self.h.set_tuning(**tune)
+        self.h.set_stream(stream.cuda_stream)
+        self.rows, self.torch, self.dev, self.cap = A.rows, torch, dev, -1
+
+    def step(self):
+        t = self.torch
+        nnz = self.h.symbolic(self.A, self.B)
+        if self.cap < nnz:
+            self.rp = t.empty(self.rows + 1, dtype=t.int32, device=self.dev)
+            self.col = t.empty(max(nnz, 1), dtype=t.int32, device=self.dev)
+            self.val = t.empty(max(nnz, 1), dtype=t.float32, device=self.dev)
+            self.cap = nnz
+        self.nnz = nnz
+        self.h.numeric(self.rp.data_ptr(), self.col.data_ptr(), self.val.data_ptr())
+
+    def close(self):
+        self.h.close()
+
+
+def timed(torch, stream, fn, steps, warmup, smi_id):
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(smi_id)
+    sampler.start()
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    return float(np.mean(ms)), sampler.stop()
+
+
+def run_suite(args, dev, stream, smi_id):
+    """ER 4096, stencil 96^3 (plain and compensated), Galerkin 64^3 (P^T A P,
+    compensated) and the 512-product batch, each: ms per step (L2 flushed
+    before every step), GFLOP/s (2 x intermediate products), algorithmic
+    bytes and their fraction of the measured HBM bandwidth, the maximum
+    relative error against an FP64 product (torch/cuSPARSE on the GPU), and
+    the clocks seen while timing."""
+    import torch
+    import spgemm_b200 as sg
+    from spgemm_b200 import workloads as W
+    peak, peak_kind = measured_peaks()
+    tune = tune_overrides(args)
+    out = {}
+
+    def prod_bytes(A, B, nnz_c):
+        p_i, a_len, b_touched, _ = product_stats(A, B)
+        o = np.zeros(A.rows, np.int64)
+        rows = np.ones(A.rows, bool)
+        base = algorithmic_bytes(rows, p_i, a_len, o, b_touched, int(p_i.sum()), with_c=False)
+        return int(p_i.sum()), base - 4 * A.rows + 4 * (A.rows + 1) + 8 * int(nnz_c)
+
+    def single(name, A, B, precision, steps, desc):
+        pr = DeviceProduct(sg, torch, dev, stream, A, B, precision, tune)
+        ms, clocks = timed(torch, stream, pr.step, steps, 3, smi_id)
+        torch.cuda.synchronize()
+        P, alg = prod_bytes(A, B, pr.nnz)
+        try:
+            ref = fp64_product(A, B)
+            err = rel_error_vs(ref, engine_keys(pr.rp, pr.col[:pr.nnz], B.cols), pr.val[:pr.nnz])
+            del ref
+        except Exception as e:  # the checker is optional; the measurement stands
+            err = {"unavailable": str(e)[:200]}
+        out[name] = {"workload": desc, "precision": "compensated" if precision else "plain",
+                     "ms_per_step": ms, "gflops": 2.0 * P / (ms / 1e3) / 1e9,
+                     "intermediate_products": P, "nnz_c": int(pr.nnz),
+                     "algorithmic_bytes": alg, "gbs": alg / (ms / 1e3) / 1e9,
+                     "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                     "max_rel_err_vs_fp64": err, "clocks": clocks}
+        pr.close()
+        torch.cuda.empty_cache()
+
+    A = W.er(4096, 8.0, 0)
+    single("er4096", A, A, sg.PLAIN, 50, "ER 4096 x 4096, 8/row, U[-1,1], C = A*A (launch-bound)")
+    A = W.stencil27(96, seed=0)
+    desc = "27-pt stencil 96^3, random sign, |v| log-uniform [1e-4, 1e4], C = A*A"
+    single("stencil96_plain", A, A, sg.PLAIN, 5, desc)
+    single("stencil96_compensated", A, A, sg.COMPENSATED, 5, desc)
+    del A
+
+    # Galerkin P^T (A P): two chained products, compensated
+    A = W.stencil27(64, values="laplace")
+    Pm = W.prolongator(64)
+    up = lambda a, t: torch.from_numpy(np.ascontiguousarray(a)).to(dev, dtype=t)
+    Ac = A.to_csc()
+    k = [up(Ac.colptr, torch.int32), up(Ac.rowidx, torch.int32), up(Ac.val, torch.float32),
+         up(Pm.rowptr, torch.int32), up(Pm.col, torch.int32), up(Pm.val, torch.float32)]
+    A_cm = sg.device_cm(k[0].data_ptr(), k[1].data_ptr(), k[2].data_ptr(), A.nnz, A.rows, A.cols, sg.COL_MAJOR)
+    P_cm = sg.device_cm(k[3].data_ptr(), k[4].data_ptr(), k[5].data_ptr(), Pm.nnz, Pm.rows, Pm.cols, sg.ROW_MAJOR)
+    PT_cm = sg.device_cm(k[3].data_ptr(), k[4].data_ptr(), k[5].data_ptr(), Pm.nnz, Pm.cols, Pm.rows, sg.COL_MAJOR)
+    h1, h2 = sg.Handle(sg.COMPENSATED), sg.Handle(sg.COMPENSATED)
+    for h in (h1, h2):
+        if tune:
+            h.set_tuning(**tune)
+        h.set_stream(stream.cuda_stream)
+    res = {}
+
+    def chain():
+        res["ap"] = h1.multiply(A_cm, P_cm)
+        res["c"] = h2.multiply(PT_cm, res["ap"])
+    ms, clocks = timed(torch, stream, chain, 10, 3, smi_id)
+    P1, P2 = h1.stats()["intermediate_products"], h2.stats()["intermediate_products"]
+    nnz_ap = h1.stats()["nnz_c"]
+    Pt = Pm.transpose()
+    # algorithmic bytes of both products: A*P, then P^T*(AP) (every row of AP touched)
+    alg = prod_bytes(A, Pm, nnz_ap)[1]
+    # check pass (untimed): the second product once more into caller buffers
+    nnz_c = h2.symbolic(PT_cm, res["ap"])
+    rp = torch.empty(Pt.rows + 1, dtype=torch.int32, device=dev)
+    col = torch.empty(max(nnz_c, 1), dtype=torch.int32, device=dev)
+    val = torch.empty(max(nnz_c, 1), dtype=torch.float32, device=dev)
+    h2.numeric(rp.data_ptr(), col.data_ptr(), val.data_ptr())
+    torch.cuda.synchronize()
+    alg += (4 * (Pt.rows + 1) + 8 * Pt.nnz + 4 * (A.rows + 1) + 8 * nnz_ap + 8 * P2 +
+            4 * (Pt.rows + 1) + 8 * nnz_c)
+    try:
+        err = rel_error_vs(fp64_chain(Pt, A, Pm), engine_keys(rp, col[:nnz_c], Pm.cols),
+                           val[:nnz_c])
+    except Exception as e:
+        err = {"unavailable": str(e)[:200]}
+    out["galerkin64"] = {"workload": "Galerkin P^T (A P), A 27-pt 64^3 (26/-1), P 2x2x2 aggregates",
+                         "precision": "compensated", "ms_per_step": ms,
+                         "gflops": 2.0 * (P1 + P2) / (ms / 1e3) / 1e9,
+                         "intermediate_products": P1 + P2, "nnz_c": int(nnz_c),
+                         "algorithmic_bytes": alg, "gbs": alg / (ms / 1e3) / 1e9,
+                         "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                         "max_rel_err_vs_fp64": err, "clocks": clocks}
+    h1.close()
+    h2.close()
+    del k, rp, col, val
+    torch.cuda.empty_cache()
+
+    # the 512-product batch: one graph replay per step against the plain loop
+    _, pairs = build_batch(args.batch_count)
+    res = measure_batch(args, dev, stream, pairs, 3, 3, 1, 0, None, smi_id)
+    hb = res["hb"]
+    ms = res["total_ms"] / 3
+    alg = res["alg_in"] + 4 * (int(res["ro"][-1]) + len(pairs)) + 8 * int(res["nnz_total"])
+    sizes = [int(np.diff(B.rowptr.astype(np.int64))[A.col].sum()) for A, B in pairs]
+    sample = sorted(set(np.random.default_rng(3).choice(len(pairs), 7, replace=False).tolist())
+                    | {int(np.argmax(sizes))})
+    errs = []
+    try:
+        for i in sample:
+            A, B = pairs[i]
+            Cb = hb.batch_copy_result(i)
+            ref = fp64_product(A, B)
+            rows = np.repeat(np.arange(Cb.rows, dtype=np.int64), np.diff(Cb.rowptr.astype(np.int64)))
+            key = torch.from_numpy(rows * B.cols + Cb.col.astype(np.int64)).cuda()
+            errs.append(rel_error_vs(ref, key, torch.from_numpy(Cb.val).cuda()))
+        err = dict(max(errs, key=lambda e: e["max_rel"]))
+        err["max_err_over_abssum"] = max(e["max_err_over_abssum"] for e in errs)
+        err["products_checked"] = len(sample)
+    except Exception as e:
+        err = {"unavailable": str(e)[:200]}
+    out["batch512"] = {"workload": f"batch of {len(pairs)} C_i = A_i*B_i (n_i log-uniform "
+                                   "[1k, 200k], Poisson(lam_i) nnz/row, lam_i ~ U[4, 32], half ER "
+                                   "/ half R-MAT), one CUDA-graph replay per step",
+                       "precision": "plain", "ms_per_step": ms,
+                       "gflops": 2.0 * res["P"] / (ms / 1e3) / 1e9,
+                       "intermediate_products": res["P"], "nnz_c": int(res["nnz_total"]),
+                       "algorithmic_bytes": alg, "gbs": alg / (ms / 1e3) / 1e9,
+                       "frac": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
+                       "plain_loop_ms": res["loop_step"],
+                       "speedup_vs_plain_loop": res["loop_step"] / ms,
+                       "autotune": {k: res["tune"][k] for k in ("tuning", "tried") if k in res["tune"]},
+                       "max_rel_err_vs_fp64": err, "clocks": res["clocks"]}
+    hb.close()
+    del res
+    torch.cuda.empty_cache()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 
@@ -591,6 +942,9 @@ def main():
         P_cm = sg.device_cm(tP[0].data_ptr(), tP[1].data_ptr(), tP[2].data_ptr(), P.nnz, P.rows, P.cols, sg.ROW_MAJOR)
         PT_cm = sg.device_cm(tP[0].data_ptr(), tP[1].data_ptr(), tP[2].data_ptr(), P.nnz, P.cols, P.rows, sg.COL_MAJOR)
         h1, h2 = sg.Handle(wl["precision"]), sg.Handle(wl["precision"])
+        for h in (h1, h2):
+            if tune_overrides(args):
+                h.set_tuning(**tune_overrides(args))
         handles = [h1, h2]
 
         def step():
@@ -607,6 +961,8 @@ def main():
         A_cm = sg.device_cm(tA[0].data_ptr(), tA[1].data_ptr(), tA[2].data_ptr(), A.nnz, A.rows, A.cols, sg.COL_MAJOR)
         B_cm = sg.device_cm(tB[0].data_ptr(), tB[1].data_ptr(), tB[2].data_ptr(), B.nnz, B.rows, B.cols, sg.ROW_MAJOR)
         h1 = sg.Handle(wl["precision"])
+        if tune_overrides(args):
+            h1.set_tuning(**tune_overrides(args))
         handles = [h1]
         out = {}
 
@@ -718,6 +1074,8 @@ def main():
         Ah = sg.Csc(A.rows, A.cols, hA[0].numpy(), hA[1].numpy(), hA[2].numpy())
         Bh = sg.Csr(B.rows, B.cols, hB[0].numpy(), hB[1].numpy(), hB[2].numpy())
         he = sg.Handle(wl["precision"])
+        if tune_overrides(args):
+            he.set_tuning(**tune_overrides(args))
         he.set_stream(stream.cuda_stream)
         h2d = sum(t.numel() * 4 for t in hA + hB)
         d2h = (A.rows + 1 + 2 * nnz_c) * 4
@@ -747,6 +1105,24 @@ def main():
         A, B = (wl["A"], wl["P"]) if args.workload == "galerkin" else wl["products"][0]
         cpu, _ = cpu_baseline(A, B, args.cpu_seconds)
 
+    # the other configurations on the same line (one GPU; R-MAT's buffers freed first)
+    configs = None
+    if rank == 0 and world == 1 and args.workload == "rmat" and not args.no_configs:
+        A, B = wl["products"][0]
+        try:
+            rmat_err = sampled_row_error(A, B, out["rowptr"], out["col"], out["val"])
+        except Exception as e:
+            rmat_err = {"unavailable": str(e)[:200]}
+        for h in handles:
+            h.close()
+        handles = []
+        out.clear()
+        keep.clear()
+        del flush
+        torch.cuda.empty_cache()
+        configs = {"rmat18": {"max_rel_err_vs_fp64": rmat_err, "precision": "plain"}}
+        configs.update(run_suite(args, dev, stream, smi_id))
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup,
@@ -759,6 +1135,8 @@ def main():
                 "roofline": roof, "pipeline": pipeline, "cpu_baseline": cpu, "e2e": e2e,
                 "clocks": clocks, "gpu_launches": launches,
                 "step_ms": step_ms}
+        if configs is not None:
+            line["configs"] = configs
         print(json.dumps(line), flush=True)
     for h in handles:
         h.close()

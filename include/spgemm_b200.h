@@ -93,9 +93,9 @@ typedef struct spgemm_tuning {
     int long_rows;        /* long rows in plain FP32 whose symbolic bitmaps were kept
                              and whose column span is at most 2^18: 0 = column
                              slices; 1 = one block per whole row, products reduced
-                             into C in L2; 2 = one block per whole row, shared-memory
-                             accumulation for rows of up to ~38K outputs (longer
-                             rows take column slices) */
+                             into C in L2; 2 (default) = one block per whole row,
+                             shared-memory accumulation for rows of up to ~38K
+                             outputs (longer rows take column slices) */
 } spgemm_tuning;
 
 /* Library version string. */

@@ -102,12 +102,13 @@ int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
   out->keep_bitmaps = t.keep_bitmaps;
   out->mid_o_min = t.mid_o_min;
   out->mid_cols = t.mid_cols;
+  out->long_rows = t.long_rows;
   return SPGEMM_OK;
 }
 
 int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
   if (!h || !in) return SPGEMM_ERR_INVALID;
-  sg::Tuning t;
+  sg::Tuning t = h->eng.tuning();
   t.warp_p_max = in->warp_p_max;
   t.warp_table_max = in->warp_table_max;
   t.warp_cap_max = in->warp_cap_max;
@@ -119,6 +120,7 @@ int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
   t.keep_bitmaps = in->keep_bitmaps ? 1 : 0;
   t.mid_o_min = in->mid_o_min;
   t.mid_cols = in->mid_cols;
+  t.long_rows = in->long_rows;
   return h->eng.set_tuning(t);
 }
 

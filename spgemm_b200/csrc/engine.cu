@@ -47,7 +47,7 @@ Tuning default_tuning() {
   t.keep_bitmaps = 1;
   t.mid_o_min = 256;
   t.mid_cols = 1 << 18;
-  t.long_rows = 0;
+  t.long_rows = 2;
   return t;
 }
 
@@ -666,67 +666,92 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
 template int Engine::launch_numeric_mode<0>(int*, float*);
 
 // Whole-row numeric path: reductions into C (long_rows = 1, any nnz_i) or
-// shared-memory accumulation (long_rows = 2, nnz_i up to the capacity that
-// one 1024-thread block's shared memory leaves after the directory). Plain
-// FP32 only, and only when the symbolic pass kept the long rows' bitmaps.
+// shared-memory accumulation (long_rows = 2): rows of up to the capacity of
+// a 512-thread block (two blocks per SM, so one block's per-row phases --
+// directory load, ranks, zeroing, copy-out -- overlap the other's products)
+// and, above it, of a 1024-thread block (one per SM). Plain FP32 only, and
+// only when the symbolic pass kept the long rows' bitmaps.
 static constexpr int ROWS_RED_THREADS = 512;
-static constexpr int ROWS_SMEM_THREADS = 1024;
-static constexpr size_t ROWS_SMEM_BUDGET = 225 * 1024;
+static constexpr size_t ROWS_SMEM_BUDGET_1 = 225 * 1024;  // one block per SM
+static constexpr size_t ROWS_SMEM_BUDGET_2 = 111 * 1024;  // two blocks per SM
 
-int Engine::rows_smem_cap() const {
-  const size_t fixed = (ROWS_SMEM_THREADS / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
-  return (int)((ROWS_SMEM_BUDGET - fixed) / sizeof(float));
+int Engine::rows_smem_cap(int threads) const {
+  const size_t fixed = (threads / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
+  const size_t budget = threads >= 1024 ? ROWS_SMEM_BUDGET_1 : ROWS_SMEM_BUDGET_2;
+  return (int)((budget - fixed) / sizeof(float));
 }
 
 int Engine::rows_cnt_max() const {
   if (precision_ != 0 || tn_.long_rows == 0 || bitmap_words_ == 0 || n_long_sym_ == 0) return 0;
-  return tn_.long_rows == 1 ? 0x7fffffff : rows_smem_cap();
+  return tn_.long_rows == 1 ? 0x7fffffff : rows_smem_cap(1024);
 }
 
 int Engine::launch_num_rows(int* c_col, float* c_val) {
   DevCounters* dc = counters_.as<DevCounters>();
   const int cnt = n_long_sym_;
   const int* rows = sym_rows_.as<int>() + (size_t)FB_LONG * m_;
-  SG_CK(lpt_order_.ensure(sizeof(int) * (size_t)cnt), "alloc row order");
+  SG_CK(lpt_order_.ensure(sizeof(int) * 2 * (size_t)cnt), "alloc row order");
   const int lb = blocks_for(cnt, 256, (long long)sms_ * 4);
-  const int cmax = rows_cnt_max();
-  prof_begin("k_lpt_hist");
-  k_lpt_hist<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
-                                      row_span_.as<int2>(), cmax, ROWS_MAX_WORDS, dc->lpt_hist);
-  SG_LAUNCHED("k_lpt_hist");
-  prof_begin("k_lpt_scatter");
-  k_lpt_scatter<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
-                                         row_span_.as<int2>(), cmax, ROWS_MAX_WORDS, dc->lpt_hist,
-                                         dc->lpt_cursor, lpt_order_.as<int>(), &dc->rows_listed);
-  SG_LAUNCHED("k_lpt_scatter");
   const Operands op = op_;
   unsigned* status = &dc->status;
-  if (tn_.long_rows == 1) {
-    constexpr int NT = ROWS_RED_THREADS;
-    const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
-    SG_CK(smem_attr(k_num_rows<NT, true>, smem), "smem attr k_num_rows");
-    prof_begin("k_num_rows");
-    k_num_rows<NT, true><<<blocks_for(cnt, 1, (long long)sms_ * 2), NT, smem, stream_>>>(
-        op, lpt_order_.as<int>(), &dc->rows_listed, &dc->row_queue, row_p_.as<long long>(),
-        c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), ROWS_MAX_WORDS, 0, c_col, c_val, status);
-    SG_LAUNCHED("k_num_rows");
-  } else {
-    constexpr int NT = ROWS_SMEM_THREADS;
-    const int cap = rows_smem_cap();
-    const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
-                        (size_t)cap * sizeof(float);
-    SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
-    prof_begin("k_num_rows");
-    k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_), NT, smem, stream_>>>(
-        op, lpt_order_.as<int>(), &dc->rows_listed, &dc->row_queue, row_p_.as<long long>(),
-        c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
-    SG_LAUNCHED("k_num_rows");
+  // (cnt_min, cnt_max] of each launch: one launch for the reduction form,
+  // two block sizes for the shared-memory form
+  const int small_cap = rows_smem_cap(512);
+  const int ranges[2][2] = {{0, tn_.long_rows == 1 ? 0x7fffffff : small_cap},
+                            {small_cap, tn_.long_rows == 1 ? 0 : rows_smem_cap(1024)}};
+  for (int g = 0; g < 2; ++g) {
+    const int cmin = ranges[g][0], cmax = ranges[g][1];
+    if (cmax <= cmin) continue;
+    int* order = lpt_order_.as<int>() + (size_t)g * cnt;
+    prof_begin("k_lpt_hist");
+    k_lpt_hist<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+                                        row_span_.as<int2>(), cmin, cmax, ROWS_MAX_WORDS,
+                                        dc->lpt_hist[g]);
+    SG_LAUNCHED("k_lpt_hist");
+    prof_begin("k_lpt_scatter");
+    k_lpt_scatter<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+                                           row_span_.as<int2>(), cmin, cmax, ROWS_MAX_WORDS,
+                                           dc->lpt_hist[g], dc->lpt_cursor[g], order,
+                                           &dc->rows_listed[g]);
+    SG_LAUNCHED("k_lpt_scatter");
+    if (tn_.long_rows == 1) {
+      constexpr int NT = ROWS_RED_THREADS;
+      const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
+      SG_CK(smem_attr(k_num_rows<NT, true>, smem), "smem attr k_num_rows");
+      prof_begin("k_num_rows");
+      k_num_rows<NT, true><<<blocks_for(cnt, 1, (long long)sms_ * 2), NT, smem, stream_>>>(
+          op, order, &dc->rows_listed[g], &dc->row_queue[g], row_p_.as<long long>(),
+          c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
+          long_slot_.as<int>(), ROWS_MAX_WORDS, 0, c_col, c_val, status);
+      SG_LAUNCHED("k_num_rows");
+    } else if (g == 0) {
+      constexpr int NT = 512;
+      const int cap = small_cap;
+      const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
+                          (size_t)cap * sizeof(float);
+      SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
+      prof_begin("k_num_rows<512>");
+      k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_ * 2), NT, smem, stream_>>>(
+          op, order, &dc->rows_listed[g], &dc->row_queue[g], row_p_.as<long long>(),
+          c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
+          long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
+      SG_LAUNCHED("k_num_rows");
+    } else {
+      constexpr int NT = 1024;
+      const int cap = rows_smem_cap(NT);
+      const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
+                          (size_t)cap * sizeof(float);
+      SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
+      prof_begin("k_num_rows<1024>");
+      k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_), NT, smem, stream_>>>(
+          op, order, &dc->rows_listed[g], &dc->row_queue[g], row_p_.as<long long>(),
+          c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
+          long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
+      SG_LAUNCHED("k_num_rows");
+    }
   }
   return 0;
 }
-template int Engine::launch_numeric_mode<1>(int*, float*);
 
 int Engine::multiply(const cm& A, const cm& B, cm* C_dev) {
   long long nnz = 0;

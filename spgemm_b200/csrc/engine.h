@@ -35,10 +35,13 @@ struct DevCounters {
   long long grand_total;
   int max_row_len;  // longest row of A (entries)
   int overflow_count;  // warp-bin rows redone by the mid / block kernels
-  int lpt_hist[32];    // whole-row numeric path: rows per work group,
-  int lpt_cursor[32];  // fill cursors of the work order,
-  int rows_listed;     // rows in the work order,
-  int row_queue;       // and the dynamic row queue
+  // whole-row numeric path, per block size (512 / 1024 threads): rows per
+  // work group, fill cursors of the work order, rows in the work order and
+  // the dynamic row queue
+  int lpt_hist[2][32];
+  int lpt_cursor[2][32];
+  int rows_listed[2];
+  int row_queue[2];
 };
 
 class Engine {
@@ -139,7 +142,7 @@ class Engine {
   // it takes for this product (0: path off), its shared-memory value
   // capacity, and its launch.
   int rows_cnt_max() const;
-  int rows_smem_cap() const;
+  int rows_smem_cap(int threads) const;
   int launch_num_rows(int* c_col, float* c_val);
   int scan_counts(const int* in, int n, long long* out);
   int check_status(unsigned st);

@@ -26,9 +26,19 @@
 //   k_num_block       long rows with few outputs: block hash + sort
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 
 namespace sg {
+
+// Functors of column-only passes may take the four columns one lane loads
+// with a 128-bit load in one call (vec4), to merge updates of the same word.
+template <class F, class = void>
+struct HasVec4 : std::false_type {};
+template <class F>
+struct HasVec4<F, std::void_t<decltype(std::declval<F&>().vec4(int4{}))>> : std::true_type {};
 
 // ---------------------------------------------------------------------------
 // Operands and tuning
@@ -181,6 +191,7 @@ __device__ __forceinline__ int compact_segments(int& bstart, int& len, float& a,
 // only columns (BITS).
 constexpr int WIN_UNROLL_VAL = 2, WIN_UNROLL_BITS = 4;
 constexpr int VEC_UNROLL_VAL = 2, VEC_UNROLL_BITS = 4;
+constexpr int VEC_INTERLEAVE_VAL = 8;  // lane-interleaved value walk: loads in flight per lane
 
 // Generate every partial product of the (<= 32) compacted segments held by
 // the warp: lane j < cnt holds B positions [bstart, bstart + len) to be
@@ -254,6 +265,31 @@ __device__ __forceinline__ void warp_run_segment_vec(int bs, int len, float a,
                                                      const float* __restrict__ b_val, F& f) {
   const int lane = lane_id();
   const int end = bs + len;
+  if constexpr (NEED_VAL) {
+    // Value passes load lane-interleaved: one warp step covers 32 * VI
+    // consecutive positions, lane l taking positions l, l + 32, ... Columns
+    // then rise with the lane, so accumulators indexed by column rank are hit
+    // on consecutive shared-memory banks (a lane holding four consecutive
+    // entries, as the 128-bit form below does, makes every access 4-way
+    // bank-conflicted on a dense slot range). Pointers are advanced once per
+    // step, so each load is one instruction with an immediate offset.
+    constexpr int VI = VEC_INTERLEAVE_VAL;
+    const int* __restrict__ pc = b_col + bs + lane;
+    const float* __restrict__ pv = b_val + bs + lane;
+    for (int q = lane; q < len; q += 32 * VI, pc += 32 * VI, pv += 32 * VI) {
+      int c[VI];
+      float v[VI];
+#pragma unroll
+      for (int u = 0; u < VI; ++u) {
+        c[u] = q + 32 * u < len ? __ldg(pc + 32 * u) : 0;
+        v[u] = q + 32 * u < len ? __ldg(pv + 32 * u) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < VI; ++u)
+        if (q + 32 * u < len) f(c[u], a, v[u]);
+    }
+    return;
+  }
   const int head = min((4 - (bs & 3)) & 3, len);
   if (lane < head) {
     const int pos = bs + lane;
@@ -275,19 +311,27 @@ __device__ __forceinline__ void warp_run_segment_vec(int bs, int len, float a,
     }
 #pragma unroll
     for (int u = 0; u < VU; ++u) {
-      f(c[u].x, a, v[u].x);
-      f(c[u].y, a, v[u].y);
-      f(c[u].z, a, v[u].z);
-      f(c[u].w, a, v[u].w);
+      if constexpr (HasVec4<F>::value) {
+        f.vec4(c[u]);
+      } else {
+        f(c[u].x, a, v[u].x);
+        f(c[u].y, a, v[u].y);
+        f(c[u].z, a, v[u].z);
+        f(c[u].w, a, v[u].w);
+      }
     }
   }
   for (; g < n4; g += 32) {
     const int4 c = __ldg(c4 + g);
     const float4 v = NEED_VAL ? __ldg(v4 + g) : make_float4(0.f, 0.f, 0.f, 0.f);
-    f(c.x, a, v.x);
-    f(c.y, a, v.y);
-    f(c.z, a, v.z);
-    f(c.w, a, v.w);
+    if constexpr (HasVec4<F>::value) {
+      f.vec4(c);
+    } else {
+      f(c.x, a, v.x);
+      f(c.y, a, v.y);
+      f(c.z, a, v.z);
+      f(c.w, a, v.w);
+    }
   }
   const int tail0 = body0 + 4 * n4;
   if (tail0 + lane < end) {
@@ -511,6 +555,21 @@ __device__ __forceinline__ void warp_expand_restricted(const Operands& op, int j
   warp_run_batch<NEED_VAL>(op, bstart, len, a, f, sc);
 }
 
+// All products of one row (whole: every entry's whole B row; otherwise the
+// slice prepared by block_restrict_row) by the nwarps warps of a block, in
+// equal per-warp ranges of the row's flattened product sequence.
+template <bool VALUES, class F>
+__device__ __forceinline__ void block_walk_row(const Operands& op, int rs, int re, bool whole,
+                                               const int* seg_start, const int* roff, int p,
+                                               F& f, SegScratch* sc, int warp, int nwarps) {
+  const int U = chunk_for(p, nwarps, 1 << 20);
+  for (int c0 = warp * U; c0 < p; c0 += nwarps * U) {
+    const int c1 = min(c0 + U, p);
+    if (whole) warp_expand_range<VALUES>(op, rs, re, c0, c1, f, sc);
+    else warp_expand_explicit<VALUES>(op, rs, re - rs, seg_start, roff, c0, c1, f, sc);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Accumulators
 // ---------------------------------------------------------------------------
@@ -550,6 +609,33 @@ struct SymHash {
 
 // Columns outside [lo, lo + width) cannot occur for validated inputs; the
 // range test keeps a malformed input from writing outside the bitmap.
+// Four columns of one lane, consecutive entries of a sorted B row (their
+// offsets x[] from the bitmap's first column): bits that fall in the same
+// 32-column word are OR-ed together first and or_word(word, mask) is called
+// once per distinct word, so a dense row costs one shared-memory atomic per
+// word instead of one per column. Returns false (nothing done) when an
+// offset lies outside [0, width): the caller then takes the columns one by
+// one with their range checks.
+template <class OrWord>
+__device__ __forceinline__ bool or_bits4(int4 c4, int lo, unsigned width, OrWord or_word) {
+  const unsigned x[4] = {(unsigned)(c4.x - lo), (unsigned)(c4.y - lo), (unsigned)(c4.z - lo),
+                         (unsigned)(c4.w - lo)};
+  if (!(x[0] < width && x[1] < width && x[2] < width && x[3] < width)) return false;
+  unsigned w = x[0] >> 5, m = 1u << (x[0] & 31);
+#pragma unroll
+  for (int q = 1; q < 4; ++q) {
+    if ((x[q] >> 5) == w) {
+      m |= 1u << (x[q] & 31);
+    } else {
+      or_word(w, m);
+      w = x[q] >> 5;
+      m = 1u << (x[q] & 31);
+    }
+  }
+  or_word(w, m);
+  return true;
+}
+
 struct SymBits {
   unsigned* bits;
   int lo;
@@ -559,6 +645,14 @@ struct SymBits {
     const unsigned c = (unsigned)(col - lo);
     if (c < width) atomicOr(bits + (c >> 5), 1u << (c & 31));
     else atomicOr(status, ST_BAD_INDEX);
+  }
+  __device__ __forceinline__ void vec4(int4 c4) {
+    if (!or_bits4(c4, lo, width, [&](unsigned w, unsigned m) { atomicOr(bits + w, m); })) {
+      (*this)(c4.x, 0.f, 0.f);
+      (*this)(c4.y, 0.f, 0.f);
+      (*this)(c4.z, 0.f, 0.f);
+      (*this)(c4.w, 0.f, 0.f);
+    }
   }
 };
 
@@ -625,6 +719,14 @@ struct LongBits {
     const unsigned c = (unsigned)(col - lo);
     if (c < width) atomicOr(&dir[c >> 5].x, 1u << (c & 31));
     else atomicOr(status, ST_BAD_INDEX);
+  }
+  __device__ __forceinline__ void vec4(int4 c4) {
+    if (!or_bits4(c4, lo, width, [&](unsigned w, unsigned m) { atomicOr(&dir[w].x, m); })) {
+      (*this)(c4.x, 0.f, 0.f);
+      (*this)(c4.y, 0.f, 0.f);
+      (*this)(c4.z, 0.f, 0.f);
+      (*this)(c4.w, 0.f, 0.f);
+    }
   }
 };
 
@@ -743,6 +845,18 @@ struct LongBitsTracked {
       atomicOr(status, ST_BAD_INDEX);
     }
   }
+  __device__ __forceinline__ void vec4(int4 c4) {
+    auto or_word = [&](unsigned w, unsigned m) {
+      const unsigned old = atomicOr(&dir[w].x, m);
+      if (old == 0u) atomicOr(l1 + (w >> 5), 1u << (w & 31));
+    };
+    if (!or_bits4(c4, lo, width, or_word)) {
+      (*this)(c4.x, 0.f, 0.f);
+      (*this)(c4.y, 0.f, 0.f);
+      (*this)(c4.z, 0.f, 0.f);
+      (*this)(c4.w, 0.f, 0.f);
+    }
+  }
 };
 
 // Output slot of `col` (only columns whose bit pass 1 set reach here, so
@@ -759,6 +873,25 @@ __device__ __forceinline__ int long_slot(const uint2* dir, int lo, int col) {
 // stores the column when its add found the slot still at +0.0 (the first
 // product of the column does, so every slot gets its column; a later store
 // after an exact cancellation writes the same index again).
+// Value functor of whole rows accumulated in shared memory: the output slot
+// is the column's rank in the row; the product that finds the slot still at
+// +0.0 (the first one does, slots start at +0.0) stores the slot's column
+// straight into C's column array, so no write-out of columns is needed.
+struct RowValCols {
+  const uint2* dir;
+  float* vals;   // shared memory, one slot per output
+  int* out_col;  // C's columns of the row (global)
+  int lo;
+  unsigned width;
+  __device__ __forceinline__ void operator()(int col, float a, float b) {
+    if ((unsigned)(col - lo) < width) {
+      const int s = long_slot(dir, lo, col);
+      const float old = atomicAdd(vals + s, __fmul_rn(a, b));
+      if (__float_as_uint(old) == 0u) __stcs(out_col + s, col);
+    }
+  }
+};
+
 struct LongValPlain {
   const uint2* dir;
   float* vals;

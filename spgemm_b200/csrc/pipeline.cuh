@@ -589,9 +589,7 @@ k_sym_long(Operands op, const int* __restrict__ rows, int nrows,
       __syncthreads();
       SymBits f{bits, w0, (unsigned)wcols, status};
       if (w0 == 0 && wcols == n) {
-        const int U = chunk_for(p, NW, 1 << 20);
-        for (int c0 = warp * U; c0 < p; c0 += NW * U)
-          warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        block_walk_row<false>(op, rs, re, true, nullptr, nullptr, p, f, sc, warp, NW);
       } else {
         const int pw = block_restrict_row(op, rs, re, w0, w0 + wcols, seg_start, roff,
                                           scan_shm, &carry_shm);
@@ -1078,19 +1076,14 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     } else {
       p = block_restrict_row(op, rs, re, sl.lo, sl.hi, seg_start, roff, scan_shm, &carry_shm);
     }
-    const int U = chunk_for(p, NW, 1 << 20);
     // pass 1: presence bits (only when the bitmap was not kept)
     if (!have_bits) {
       if (SPARSE) {
         LongBitsTracked f{dir, l1, sl.lo, (unsigned)(sl.hi - sl.lo), status};
-        for (int c0 = warp * U; c0 < p; c0 += NW * U)
-          warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
+        block_walk_row<false>(op, rs, re, true, seg_start, roff, p, f, sc, warp, NW);
       } else {
         LongBits f{dir, sl.lo, (unsigned)(sl.hi - sl.lo), status};
-        for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-          if (whole) warp_expand_range<false>(op, rs, re, c0, min(c0 + U, p), f, sc);
-          else warp_expand_explicit<false>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
-        }
+        block_walk_row<false>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
       }
       __syncthreads();
     }
@@ -1136,22 +1129,13 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     // value pass
     if (MODE == 1 && pair) {
       LongValTwoSum f{dir, reinterpret_cast<float2*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
-        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
-      }
+      block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
     } else if (MODE == 0) {
       LongValPlain f{dir, reinterpret_cast<float*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
-        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
-      }
+      block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
     } else {
       LongValF64 f{dir, reinterpret_cast<double*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U) {
-        if (whole) warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
-        else warp_expand_explicit<true>(op, rs, re - rs, seg_start, roff, c0, min(c0 + U, p), f, sc);
-      }
+      block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
     }
     __syncthreads();
     // write-out: values and columns are already in output order
@@ -1183,21 +1167,23 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
 // Work order of the long rows: grouped by floor(log2 P_i), heaviest group
 // first, so that on the dynamic row queue of k_num_rows the longest rows
 // start first and the short ones fill in at the end (longest-processing-time
-// first, to a factor of two). Only the rows whole_row_path() accepts are listed.
+// first, to a factor of two). Only the rows with more than cnt_min outputs
+// that whole_row_path(cnt_max) accepts are listed.
 constexpr int LPT_GROUPS = 32;
 
 __device__ __forceinline__ int lpt_group(long long p) { return 63 - __clzll(p > 0 ? p : 1); }
 
 __global__ void __launch_bounds__(256)
 k_lpt_hist(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
-           const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_max,
-           int max_words, int* __restrict__ hist) {
+           const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_min,
+           int cnt_max, int max_words, int* __restrict__ hist) {
   __shared__ int h[LPT_GROUPS];
   if (threadIdx.x < LPT_GROUPS) h[threadIdx.x] = 0;
   __syncthreads();
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
     const int i = rows[r];
-    if (whole_row_path(c_cnt[i], row_span[i], cnt_max, max_words))
+    const int o = c_cnt[i];
+    if (o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words))
       atomicAdd(&h[min(lpt_group(row_p[i]), LPT_GROUPS - 1)], 1);
   }
   __syncthreads();
@@ -1208,8 +1194,8 @@ k_lpt_hist(const int* __restrict__ rows, int nrows, const long long* __restrict_
 // order: the listed rows, heaviest group first; *nlisted: their count.
 __global__ void __launch_bounds__(256)
 k_lpt_scatter(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
-              const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_max,
-              int max_words, const int* __restrict__ hist, int* __restrict__ cursor,
+              const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_min,
+              int cnt_max, int max_words, const int* __restrict__ hist, int* __restrict__ cursor,
               int* __restrict__ order, int* __restrict__ nlisted) {
   __shared__ int base[LPT_GROUPS];
   if (threadIdx.x == 0) {
@@ -1223,7 +1209,8 @@ k_lpt_scatter(const int* __restrict__ rows, int nrows, const long long* __restri
   __syncthreads();
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
     const int i = rows[r];
-    if (whole_row_path(c_cnt[i], row_span[i], cnt_max, max_words)) {
+    const int o = c_cnt[i];
+    if (o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words)) {
       const int g = min(lpt_group(row_p[i]), LPT_GROUPS - 1);
       order[base[g] + atomicAdd(cursor + g, 1)] = i;
     }
@@ -1264,10 +1251,12 @@ struct RowValSmem {
 // every 32-column word); every product then adds into its final position
 // out0 + rank(column), so the row is produced in column order with no
 // column slicing and no sort. RED: values accumulate in C itself (zeroed
-// first; the row's value range stays in L2 while the block works on it);
-// otherwise in shared memory (rows of at most `cap` outputs), copied out at
-// the end. Columns are written from the directory. Shared memory: per-warp
-// scratch | directory uint2[dir_words] | (not RED) values float[cap].
+// first; the row's value range stays in L2 while the block works on it) and
+// the columns are written from the directory; otherwise values accumulate in
+// shared memory (rows of at most `cap` outputs) and are copied out at the
+// end, and each column is stored into C by the product that first touches
+// its slot. Shared memory: per-warp scratch | directory uint2[dir_words] |
+// (not RED) values float[cap].
 template <int NT, bool RED>
 __global__ void __launch_bounds__(NT, NT >= 1024 ? 1 : 2)
 k_num_rows(Operands op, const int* __restrict__ order, const int* __restrict__ nrows_p,
@@ -1318,31 +1307,31 @@ k_num_rows(Operands op, const int* __restrict__ order, const int* __restrict__ n
     __syncthreads();  // ranks and zeroed values visible to the whole block
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     const int p = (int)row_p[i];
-    const int U = chunk_for(p, NW, 1 << 20);
     const unsigned width = (unsigned)(sp.y + 1 - lo);
     if (RED) {
       RowValRed f{dir, c_val + out0, lo, width};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U)
-        warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+      block_walk_row<true>(op, rs, re, true, nullptr, nullptr, p, f, sc, warp, NW);
     } else {
-      RowValSmem f{dir, vals, lo, width};
-      for (int c0 = warp * U; c0 < p; c0 += NW * U)
-        warp_expand_range<true>(op, rs, re, c0, min(c0 + U, p), f, sc);
+      RowValCols f{dir, vals, c_col + out0, lo, width};
+      block_walk_row<true>(op, rs, re, true, nullptr, nullptr, p, f, sc, warp, NW);
     }
     __syncthreads();
-    // columns (and shared-memory values) in rank order, one directory word
-    // per thread at a time
-    for (int w = threadIdx.x; w < nw; w += NT) {
-      const uint2 d = dir[w];
-      unsigned b = d.x;
-      int pos = (int)d.y;
-      while (b) {
-        const int bit = __ffs(b) - 1;
-        b &= b - 1u;
-        __stcs(c_col + out0 + pos, lo + 32 * w + bit);
-        if (!RED) __stcs(c_val + out0 + pos, vals[pos]);
-        ++pos;
+    if (RED) {
+      // columns in rank order from the directory, one word per thread at a time
+      for (int w = threadIdx.x; w < nw; w += NT) {
+        const uint2 d = dir[w];
+        unsigned b = d.x;
+        int pos = (int)d.y;
+        while (b) {
+          const int bit = __ffs(b) - 1;
+          b &= b - 1u;
+          __stcs(c_col + out0 + pos, lo + 32 * w + bit);
+          ++pos;
+        }
       }
+    } else {
+      // the columns were stored at first touch; values in output order
+      block_store_aligned<NT>(c_val + out0, cnt, [&](int t) { return vals[t]; });
     }
     __syncthreads();
   }

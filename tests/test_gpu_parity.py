@@ -87,7 +87,16 @@ def test_rmat_all_bins():
     _, _, stats = check(A, A)
     assert stats["rows_per_symbolic_bin"][9] > 0, stats   # long rows
     assert stats["rows_per_symbolic_bin"][8] > 0, stats   # fused span bitmap
-    assert stats["rows_per_numeric_bin"][8] > 0, stats    # column slices
+    assert stats["long_row_slices"] == 0, stats           # every long row taken whole
+    # with the whole-row kernel off, long rows take column slices
+    with sg.Handle() as h:
+        h.set_tuning(long_rows=0)
+        C = h.multiply_host(A.to_csc(), A)
+        st0 = h.stats()
+    ref = ref_product(A, A)
+    assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+    assert_values_close(C.val, ref, plain_tolerance(ref))
+    assert st0["rows_per_numeric_bin"][8] > 0, st0        # column slices
 
 
 def test_rmat_all_bins_compensated():
@@ -154,7 +163,7 @@ def test_repeat_calls_reuse_workspace():
 
 TUNINGS = [
     dict(keep_bitmaps=0),                                   # numeric rebuilds long-row bitmaps
-    dict(slice_cap=2048, slice_cols=8192),                  # many column slices per long row
+    dict(slice_cap=2048, slice_cols=8192, long_rows=0),     # many column slices per long row
     dict(warp_p_max=0),                                     # no fused warp rows: block / bitmap
     dict(warp_table_max=64),                                # most warp rows overflow and are redone
     dict(warp_table_max=1024, warp_cap_max=4096),           # large warp tables
