@@ -59,6 +59,8 @@ def parse_args():
                    help="batch: timed passes of the one-product-per-launch loop")
     p.add_argument("--no-autotune", action="store_true")
     p.add_argument("--scale", type=int, default=18, help="R-MAT scale (default 18)")
+    p.add_argument("--grid", type=int, default=96,
+                   help="stencil grid side (default 96; smaller grids for profiling)")
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
@@ -91,11 +93,12 @@ def build_workload(args):
                 "config": {"workload": f"R-MAT 2^{args.scale} ef16 (0.57,0.19,0.19,0.05) dedup, "
                                        "values U(0,1], C = A*A", "rows": A.rows, "nnz_a": A.nnz}}
     if args.workload in ("stencil", "stencil-comp"):
-        A = W.stencil27(96, seed=0)
+        g = args.grid
+        A = W.stencil27(g, seed=0)
         comp = args.workload == "stencil-comp"
-        return {"name": "stencil96_27pt_AxA" + ("_compensated" if comp else ""),
+        return {"name": f"stencil{g}_27pt_AxA" + ("_compensated" if comp else ""),
                 "products": [(A, A)], "precision": 1 if comp else 0,
-                "config": {"workload": "27-point stencil 96^3, random sign, |v| log-uniform "
+                "config": {"workload": f"27-point stencil {g}^3, random sign, |v| log-uniform "
                                        f"[1e-4,1e4], C = A*A, {'compensated' if comp else 'plain'} FP32",
                            "rows": A.rows, "nnz_a": A.nnz}}
     if args.workload == "er":
@@ -139,6 +142,7 @@ def product_stats(A, B):
 # Mirrors of the engine's default bin rules (kernels.cuh), used only to
 # attribute algorithmic bytes to the kernel that processed each row.
 LONG_P, WARP_CAP, WARP_TMAX, MID_COLS, LONG_O, MID_O = 4096, 2048, 256, 1 << 18, 4096, 256
+ESC_P_MIN, ESC_SPAN_MIN = 0, 0  # rows outside the warp bins merged by sorting
 # output capacities of the whole-row kernel's two block sizes (engine.cu:
 # (shared-memory budget - per-warp scratch - directory) / 4 bytes)
 ROWS_CAP_512 = (111 * 1024 - 16 * 388 - 8193 * 8) // 4
@@ -149,7 +153,9 @@ def first_bin(p, cap, span):
     lg = np.ceil(np.log2(np.maximum(cap + cap // 4 + 1, 1))).astype(np.int64)
     warp = np.clip(lg, 6, int(np.log2(WARP_TMAX))) - 6
     blk = np.maximum(np.ceil(np.log2(np.maximum(2 * cap, 1))).astype(np.int64), 11) - 11 + 5
-    b = np.where(cap <= WARP_CAP, warp, np.where(span <= MID_COLS, 8, blk))
+    esc = (p > ESC_P_MIN) & (span > ESC_SPAN_MIN)
+    esc_bin = np.where(p <= 1024, 10, np.where(p <= 2048, 11, 12))
+    b = np.where(cap <= WARP_CAP, warp, np.where(esc, esc_bin, np.where(span <= MID_COLS, 8, blk)))
     b = np.where(p > LONG_P, 9, b)
     return np.where(p <= 0, -1, b)
 
@@ -175,6 +181,9 @@ def kernel_rows(name, p_i, o_i, span, n):
         return long_rows & (o_i > MID_O) & (o_i <= LONG_O) & (span <= MID_COLS), True
     if name == "k_fused_mid":
         return fb == 8, True
+    m = re.match(r"k_fused_esc<(\d+)>", name)
+    if m:
+        return fb == {128: 10, 256: 11, 512: 12}[int(m.group(1))], True
     m = re.match(r"k_fused_(warp|block)<(\d+)>", name)
     if m:
         lg = int(m.group(2))

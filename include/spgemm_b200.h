@@ -58,7 +58,9 @@ typedef struct spgemm_stats {
     long long nnz_c;                   /* exact nnz(C) */
     int rows_per_symbolic_bin[16];     /* rows per first-pass bin: 0..4 warp hash
                                           (64..1024 slots), 5..7 block hash
-                                          (2048..8192), 8 span bitmap, 9 long */
+                                          (2048..8192), 8 span bitmap, 9 long,
+                                          10..12 sorted (rows of <= 1024, 2048,
+                                          4096 products) */
     int rows_per_numeric_bin[16];      /* long rows per numeric bin: 4..7 block
                                           hash, 8 column slices, 9 span bitmap */
     int long_row_slices;               /* column slices of the long-row path */
@@ -95,7 +97,15 @@ typedef struct spgemm_tuning {
                              slices; 1 = one block per whole row, products reduced
                              into C in L2; 2 (default) = one block per whole row,
                              shared-memory accumulation for rows of up to ~38K
-                             outputs (longer rows take column slices) */
+                             outputs (longer rows take column slices); 3 = as 2,
+                             with the longer rows reduced into C in L2 */
+    int esc_p_min;        /* rows outside the warp bins (column bound above
+                             warp_cap_max) with esc_p_min < P_i <= long_p and a
+                             column span above esc_span_min are merged by
+                             sorting their products (one block per row) instead
+                             of the span bitmap / block hash; esc_p_min >=
+                             long_p turns this off */
+    int esc_span_min;
 } spgemm_tuning;
 
 /* Library version string. */
@@ -146,6 +156,14 @@ int spgemm_multiply_host(spgemm_handle_t handle, cm A_host, cm B_host,
 int spgemm_multiply_host_to(spgemm_handle_t handle, cm A_host, cm B_host,
                             int* c_rowptr, int* c_colidx, float* c_val,
                             long long capacity, long long* nnz_c);
+/* The two host-buffer entry points above copy C back in pieces of about
+ * `bytes` of C each (row ranges; at most 16 pieces): the numeric pass runs
+ * piece by piece and each piece's device-to-host copy, on a second stream of
+ * the handle, overlaps the computation of the pieces after it. Default
+ * 64 MiB; 0 copies C in one piece after the whole product. Pinned host
+ * arrays let the copies run asynchronously; with pageable arrays every copy
+ * still waits only for its own piece. */
+int spgemm_set_copy_chunk(spgemm_handle_t handle, long long bytes);
 
 /* Batched products. The reference multiplies one pair per process
  * (src/main.cu:31-37 drives src/mm.cu once); these entry points run `count`

@@ -62,7 +62,7 @@ class Tuning(C.Structure):
                 ("warp_cap_max", C.c_int), ("long_p", C.c_int), ("long_o_num", C.c_int),
                 ("slice_cap", C.c_int), ("slice_cols", C.c_int), ("sym_window", C.c_int),
                 ("keep_bitmaps", C.c_int), ("mid_o_min", C.c_int), ("mid_cols", C.c_int),
-                ("long_rows", C.c_int)]
+                ("long_rows", C.c_int), ("esc_p_min", C.c_int), ("esc_span_min", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -101,6 +101,7 @@ def lib():
         L.spgemm_multiply_host.argtypes = [vp, CM, CM, C.POINTER(CM)]
         L.spgemm_multiply_host_to.argtypes = [vp, CM, CM, ip, ip, fp, C.c_longlong,
                                               C.POINTER(C.c_longlong)]
+        L.spgemm_set_copy_chunk.argtypes = [vp, C.c_longlong]
         L.spgemm_get_result.argtypes = [C.POINTER(CM)]
         L.spgemm_set_verbose.argtypes = [C.c_int]
         L.spgemm_set_exit_on_error.argtypes = [C.c_int]
@@ -231,7 +232,7 @@ class Handle:
         s = Stats()
         self._check(lib().spgemm_get_stats(self._h, C.byref(s)))
         return {"intermediate_products": s.intermediate_products, "nnz_c": s.nnz_c,
-                "rows_per_symbolic_bin": list(s.rows_per_symbolic_bin)[:10],
+                "rows_per_symbolic_bin": list(s.rows_per_symbolic_bin)[:13],
                 "warp_overflow_rows": s.warp_overflow_rows,
                 "rows_per_numeric_bin": list(s.rows_per_numeric_bin)[:10],
                 "long_row_slices": s.long_row_slices, "kernel_launches": s.kernel_launches}
@@ -250,6 +251,11 @@ class Handle:
                 raise KeyError(k)
             setattr(t, k, int(v))
         self._check(lib().spgemm_set_tuning(self._h, C.byref(t)))
+
+    def set_copy_chunk(self, nbytes: int):
+        """Bytes of C per device-to-host piece of the host-buffer calls
+        (0: one piece after the whole product)."""
+        self._check(lib().spgemm_set_copy_chunk(self._h, int(nbytes)))
 
     def set_profiling(self, on: bool = True):
         self._check(lib().spgemm_set_profiling(self._h, 1 if on else 0))

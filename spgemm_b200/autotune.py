@@ -1,8 +1,8 @@
 """Autotuner of the batched path.
 
-Picks the tuning (include/spgemm_b200.h `spgemm_tuning`: bin thresholds of
-the warp-per-row bins, warp hash-table sizes, the long-row threshold, the
-mid-row bitmap width) that runs a given batch fastest on this GPU. Each
+Picks the tuning (include/spgemm_b200.h `spgemm_tuning`: the smallest row
+that is merged by sorting, bin thresholds of the warp-per-row bins, warp
+hash-table sizes, the long-row threshold, the mid-row bitmap width) that runs a given batch fastest on this GPU. Each
 candidate is planned (spgemm_batch_plan) and then timed as replays of the
 batch's CUDA graph (spgemm_batch_execute), so the choice reflects exactly
 the work a serving loop repeats. The search is coordinate descent from the
@@ -22,7 +22,8 @@ from pathlib import Path
 SEARCH = [
     ("warp_table_max", [256, 512, 1024]),
     ("warp_p_max", [1024, 2048, 4096]),
-    ("warp_cap_max", [512, 1024, 2048]),
+    ("warp_cap_max", [128, 256, 512, 1024, 2048]),  # rows above: sorted (or mid / block)
+    ("esc_p_min", [0, 4096]),                        # 4096: no sorted rows
     ("long_p", [2048, 4096]),
     ("mid_cols", [0, 1 << 16, 1 << 18]),
 ]

@@ -1,10 +1,12 @@
 // C ABI of the engine (include/spgemm_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "../../include/spgemm_b200.h"
 #include "context.h"
@@ -40,6 +42,87 @@ int stage_matrix(sg::Engine& E, const cm& H, int slot, cm* D) {
   if (int r = copy_in(E, E.stage(3 * slot + 2), H.val, sizeof(float) * (size_t)H.nnz, &p)) return r;
   D->val = static_cast<float*>(p);
   return SPGEMM_OK;
+}
+
+// Numeric pass of the current symbolic result into the engine-owned C,
+// copied to the host arrays piece by piece: the rows are cut into pieces of
+// about h->copy_chunk bytes of C (at most MAX_PIECES), each piece is
+// computed on the engine's stream and, once its event has fired, copied on
+// the handle's copy stream while the later pieces compute. All pieces are
+// enqueued before the first copy, so with pageable host memory (where a
+// device-to-host cudaMemcpyAsync returns only when done) the computation
+// still runs ahead of the copies. The row pointers come last.
+int numeric_to_host(spgemm_handle_t h, int* c_rowptr, int* c_colidx, float* c_val) {
+  sg::Engine& E = h->eng;
+  cm C;
+  if (int r = E.owned_output(&C)) return r;
+  const int m = C.num_rows;
+  const long long nnz = E.nnz_c();
+  const long long bytes = 8 * nnz;
+  const long long chunk = h->copy_chunk > 0 ? h->copy_chunk : bytes;
+  int pieces = (int)std::min<long long>(spgemm_context::MAX_PIECES,
+                                        std::max<long long>(1, (bytes + chunk - 1) / std::max(chunk, 1ll)));
+  if (m == 0) pieces = 1;
+  std::vector<long long> rp;
+  std::vector<int> bounds(1, 0);
+  if (pieces > 1) {
+    rp.resize((size_t)m + 1);
+    if (int r = E.rowptr64_to_host(rp.data())) return r;
+    for (int j = 1; j < pieces; ++j) {
+      const long long target = nnz * j / pieces;
+      int r = (int)(std::lower_bound(rp.begin(), rp.end(), target) - rp.begin());
+      r = std::min(std::max(r, bounds.back()), m);
+      bounds.push_back(r);
+    }
+  }
+  bounds.push_back(m);
+  cudaStream_t s = E.stream();
+  cudaError_t e = cudaSuccess;
+  if (pieces > 1 && !h->copy_stream) {
+    e = cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return E.cuda_fail(e, "create copy stream");
+  }
+  for (int j = 0; j < pieces; ++j) {
+    if (int r = E.numeric_rows(C.idx, C.val, bounds[j], bounds[j + 1])) return r;
+    if (pieces > 1) {
+      if (!h->piece_done[j]) {
+        e = cudaEventCreateWithFlags(&h->piece_done[j], cudaEventDisableTiming);
+        if (e != cudaSuccess) return E.cuda_fail(e, "create piece event");
+      }
+      e = cudaEventRecord(h->piece_done[j], s);
+      if (e != cudaSuccess) return E.cuda_fail(e, "record piece event");
+    }
+  }
+  // copies: one piece after another on the copy stream (the whole of C on
+  // the engine's stream when there is a single piece)
+  for (int j = 0; j < pieces && e == cudaSuccess; ++j) {
+    const long long e0 = pieces > 1 ? rp[bounds[j]] : 0;
+    const long long e1 = pieces > 1 ? rp[bounds[j + 1]] : nnz;
+    if (e1 <= e0) continue;
+    cudaStream_t cs = s;
+    if (pieces > 1) {
+      cs = h->copy_stream;
+      e = cudaStreamWaitEvent(cs, h->piece_done[j], 0);
+    }
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c_colidx + e0, C.idx + e0, sizeof(int) * (size_t)(e1 - e0),
+                          cudaMemcpyDeviceToHost, cs);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(c_val + e0, C.val + e0, sizeof(float) * (size_t)(e1 - e0),
+                          cudaMemcpyDeviceToHost, cs);
+  }
+  int r = e == cudaSuccess ? E.numeric_rowptr(C.ptr) : E.cuda_fail(e, "copy C to host");
+  if (r == SPGEMM_OK) {
+    e = cudaMemcpyAsync(c_rowptr, C.ptr, sizeof(int) * ((size_t)m + 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) r = E.cuda_fail(e, "copy C row pointers to host");
+  }
+  // the host arrays stay in use until the copy stream is idle
+  if (h->copy_stream) {
+    e = cudaStreamSynchronize(h->copy_stream);
+    if (e != cudaSuccess && r == SPGEMM_OK) r = E.cuda_fail(e, "copy C to host");
+  }
+  return r;
 }
 
 }  // namespace
@@ -103,6 +186,8 @@ int spgemm_get_tuning(spgemm_handle_t h, spgemm_tuning* out) {
   out->mid_o_min = t.mid_o_min;
   out->mid_cols = t.mid_cols;
   out->long_rows = t.long_rows;
+  out->esc_p_min = t.esc_p_min;
+  out->esc_span_min = t.esc_span_min;
   return SPGEMM_OK;
 }
 
@@ -121,6 +206,8 @@ int spgemm_set_tuning(spgemm_handle_t h, const spgemm_tuning* in) {
   t.mid_o_min = in->mid_o_min;
   t.mid_cols = in->mid_cols;
   t.long_rows = in->long_rows;
+  t.esc_p_min = in->esc_p_min;
+  t.esc_span_min = in->esc_span_min;
   return h->eng.set_tuning(t);
 }
 
@@ -219,18 +306,12 @@ int spgemm_multiply_host_to(spgemm_handle_t h, cm A_host, cm B_host, int* c_rowp
   if (nnz_c) *nnz_c = nnz;
   if (nnz > capacity || !c_rowptr || (nnz > 0 && (!c_colidx || !c_val)))
     return E.fail(SPGEMM_ERR_TOO_LARGE, "output capacity below nnz(C)");
-  cm C;
-  if (int r = E.multiply_numeric_owned(&C)) return r;
-  cudaStream_t s = E.stream();
-  cudaError_t e;
-  e = cudaMemcpyAsync(c_rowptr, C.ptr, sizeof(int) * ((size_t)C.num_rows + 1),
-                      cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && nnz > 0)
-    e = cudaMemcpyAsync(c_colidx, C.idx, sizeof(int) * (size_t)nnz, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && nnz > 0)
-    e = cudaMemcpyAsync(c_val, C.val, sizeof(float) * (size_t)nnz, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return E.cuda_fail(e, "copy C to host");
+  return numeric_to_host(h, c_rowptr, c_colidx, c_val);
+}
+
+int spgemm_set_copy_chunk(spgemm_handle_t h, long long bytes) {
+  if (!h || bytes < 0) return SPGEMM_ERR_INVALID;
+  h->copy_chunk = bytes;
   return SPGEMM_OK;
 }
 
@@ -240,31 +321,24 @@ int spgemm_multiply_host(spgemm_handle_t h, cm A_host, cm B_host, cm* C_host) {
   cm A, B;
   if (int r = stage_matrix(E, A_host, 0, &A)) return r;
   if (int r = stage_matrix(E, B_host, 1, &B)) return r;
-  cm C;
-  if (int r = E.multiply(A, B, &C)) return r;
+  long long nnz = 0;
+  if (int r = E.symbolic(A, B, &nnz)) return r;
+  if (nnz > 2147483647ll) return E.fail(SPGEMM_ERR_OVERFLOW, "nnz(C) exceeds the int32 range of cm");
   cm out;
-  out.num_rows = C.num_rows;
-  out.num_cols = C.num_cols;
-  out.nnz = C.nnz;
+  out.num_rows = A.num_rows;
+  out.num_cols = B.num_cols;
+  out.nnz = (int)nnz;
   out.type = ROW_MAJOR;
-  out.ptr = static_cast<int*>(malloc(sizeof(int) * ((size_t)C.num_rows + 1)));
-  out.idx = static_cast<int*>(malloc(sizeof(int) * (size_t)(C.nnz > 0 ? C.nnz : 1)));
-  out.val = static_cast<float*>(malloc(sizeof(float) * (size_t)(C.nnz > 0 ? C.nnz : 1)));
+  out.ptr = static_cast<int*>(malloc(sizeof(int) * ((size_t)out.num_rows + 1)));
+  out.idx = static_cast<int*>(malloc(sizeof(int) * (size_t)(nnz > 0 ? nnz : 1)));
+  out.val = static_cast<float*>(malloc(sizeof(float) * (size_t)(nnz > 0 ? nnz : 1)));
   if (!out.ptr || !out.idx || !out.val) {
     free(out.ptr); free(out.idx); free(out.val);
     return E.fail(SPGEMM_ERR_ALLOC, "host allocation of C failed");
   }
-  cudaStream_t s = E.stream();
-  cudaError_t e = cudaMemcpyAsync(out.ptr, C.ptr, sizeof(int) * ((size_t)C.num_rows + 1),
-                                  cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && C.nnz > 0)
-    e = cudaMemcpyAsync(out.idx, C.idx, sizeof(int) * (size_t)C.nnz, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && C.nnz > 0)
-    e = cudaMemcpyAsync(out.val, C.val, sizeof(float) * (size_t)C.nnz, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) {
+  if (int r = numeric_to_host(h, out.ptr, out.idx, out.val)) {
     free(out.ptr); free(out.idx); free(out.val);
-    return E.cuda_fail(e, "copy C to host");
+    return r;
   }
   *C_host = out;
   return SPGEMM_OK;

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 
+#include "esc.cuh"
 #include "pipeline.cuh"
 
 namespace sg {
@@ -48,6 +49,8 @@ Tuning default_tuning() {
   t.mid_o_min = 256;
   t.mid_cols = 1 << 18;
   t.long_rows = 2;
+  t.esc_p_min = 0;
+  t.esc_span_min = 0;
   return t;
 }
 
@@ -150,7 +153,8 @@ int Engine::set_tuning(const Tuning& t) {
     return fail(1, "tuning: slice_cap must be 0 (auto) or >= 2048");
   if (t.mid_o_min < 0 || t.mid_cols < 0 || t.mid_cols > (1 << 18))
     return fail(1, "tuning: mid_o_min >= 0 and 0 <= mid_cols <= 2^18");
-  if (t.long_rows < 0 || t.long_rows > 2) return fail(1, "tuning: long_rows must be 0, 1 or 2");
+  if (t.long_rows < 0 || t.long_rows > 3) return fail(1, "tuning: long_rows must be 0..3");
+  if (t.esc_p_min < 0 || t.esc_span_min < 0) return fail(1, "tuning: esc_p_min, esc_span_min >= 0");
   tn_ = t;
   return 0;
 }
@@ -375,7 +379,9 @@ int Engine::symbolic_pass(long long* nnz_c) {
   // output capacity of one big slice: what the shared-memory budget leaves
   Tuning tr = tn_;
   {
-    const size_t vb = (precision_ == 1 ? 8 : 4) + sizeof(int);  // value and column per slot
+    // per slot: the value, and (compensated) its column; plain slices store
+    // columns straight into C
+    const size_t vb = precision_ == 1 ? 8 + sizeof(int) : 4;
     const size_t fixed = (BIG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes();
     long long cap = (long long)((BIG_SMEM_BUDGET - fixed) / vb);
     cap = std::min<long long>(cap, 1 << 20);
@@ -486,7 +492,8 @@ int Engine::launch_fused() {
                                          toff, c_cnt, t_col, t_val, mid_rows,                  \
                                          &dc->fb_count[FB_MID], big_rows,                      \
                                          &dc->fb_count[FB_BLOCK0 + 2], tn_.mid_cols,           \
-                                         &dc->overflow_count);                                 \
+                                         rows + (size_t)FB_ESC0 * m, &dc->fb_count[FB_ESC0],   \
+                                         tn_, row_p, &dc->overflow_count);                     \
       SG_LAUNCHED("k_fused_warp");                                                             \
     }                                                                                          \
   }
@@ -506,7 +513,7 @@ int Engine::launch_fused() {
     k_num_long<MODE, MID_THREADS, true><<<grid, MID_THREADS, smem, stream_>>>(
         op, nullptr, 0, row_p, dir_words, cap, restrict_scratch_.as<int>(), 0,
         bitmaps_.as<unsigned>(), 0, long_slot_.as<int>(), t_col, t_val, status, mid_rows,
-        &dc->fb_count[FB_MID], row_span_.as<int2>(), toff, c_cnt);
+        &dc->fb_count[FB_MID], row_span_.as<int2>(), toff, c_cnt, 0, m);
     SG_LAUNCHED("k_fused_mid");
   }
 #define SG_FUSED_BLOCK(L, NT)                                                                 \
@@ -526,23 +533,79 @@ int Engine::launch_fused() {
   }
   SG_FUSED_BLOCK(11, 256) SG_FUSED_BLOCK(12, 256) SG_FUSED_BLOCK(13, 512)
 #undef SG_FUSED_BLOCK
+  // sorted rows (expand, sort, compress), one block per row; the lists may
+  // also hold warp rows that overflowed their tables
+#define SG_FUSED_ESC(Q, NT, PER_SM)                                                           \
+  {                                                                                            \
+    const int b = FB_ESC0 + Q, cnt = fb_counts_[b] + overflow_bound;                           \
+    if (cnt > 0) {                                                                             \
+      const size_t smem = esc_smem_bytes<NT, MODE>();                                          \
+      SG_CK(smem_attr(k_fused_esc<NT, MODE>, smem), "smem attr k_fused_esc");                  \
+      prof_begin("k_fused_esc<" #NT ">");                                                      \
+      k_fused_esc<NT, MODE><<<blocks_for(cnt, 1, (long long)sms_ * (PER_SM)), NT, smem,        \
+                              stream_>>>(op, rows + (size_t)b * m, &dc->fb_count[b], row_p,    \
+                                         toff, row_span_.as<int2>(), c_cnt, t_col, t_val,      \
+                                         status);                                              \
+      SG_LAUNCHED("k_fused_esc");                                                              \
+    }                                                                                          \
+  }
+  SG_FUSED_ESC(0, 128, 8) SG_FUSED_ESC(1, 256, 4) SG_FUSED_ESC(2, 512, MODE ? 1 : 2)
+#undef SG_FUSED_ESC
   return 0;
 }
 
 template int Engine::launch_fused<0>();
 template int Engine::launch_fused<1>();
 
-int Engine::numeric_values(int* c_col, float* c_val) {
+int Engine::numeric_values(int* c_col, float* c_val) { return numeric_rows(c_col, c_val, 0, m_); }
+
+int Engine::numeric_rows(int* c_col, float* c_val, int r0, int r1) {
   if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
   if (nnz_c_ > 0 && (!c_col || !c_val)) return fail(1, "null output pointer");
-  if (m_ > 0 && temp_total_ > 0) {
+  if (r0 < 0 || r1 > m_ || r0 > r1) return fail(1, "numeric: row range outside [0, m]");
+  if (r1 > r0 && temp_total_ > 0) {
     prof_begin("k_copy_fused");
-    k_copy_fused<<<blocks_for((long long)m_, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
-        m_, tcap_.as<int>(), toff_.as<long long>(), c_cnt_.as<int>(), c_rowptr64_.as<long long>(),
-        t_col_.as<int>(), t_val_.as<float>(), c_col, c_val);
+    k_copy_fused<<<blocks_for((long long)(r1 - r0), 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+        r0, r1, tcap_.as<int>(), toff_.as<long long>(), c_cnt_.as<int>(),
+        c_rowptr64_.as<long long>(), t_col_.as<int>(), t_val_.as<float>(), c_col, c_val);
     SG_LAUNCHED("k_copy_fused");
   }
-  return launch_numeric_bins(c_col, c_val);
+  return launch_numeric_bins(c_col, c_val, r0, r1);
+}
+
+int Engine::numeric_rowptr(int* c_rowptr) {
+  if (!have_sym_) return fail(5, "numeric called without a successful symbolic pass");
+  if (!c_rowptr) return fail(1, "null output pointer");
+  prof_begin("k_rowptr_to_i32");
+  k_rowptr_to_i32<<<blocks_for(m_ + 1, 256, (long long)sms_ * 16), 256, 0, stream_>>>(
+      c_rowptr64_.as<long long>(), m_ + 1, c_rowptr);
+  SG_LAUNCHED("k_rowptr_to_i32");
+  return finish_numeric();
+}
+
+int Engine::owned_output(cm* C_dev) {
+  if (!have_sym_) return fail(5, "output requested without a successful symbolic pass");
+  const long long nnz = nnz_c_;
+  SG_CK(out_rowptr_.ensure(sizeof(int) * ((size_t)m_ + 1)), "alloc C row pointers");
+  SG_CK(out_col_.ensure(sizeof(int) * (size_t)std::max(nnz, 1ll)), "alloc C columns");
+  SG_CK(out_val_.ensure(sizeof(float) * (size_t)std::max(nnz, 1ll)), "alloc C values");
+  C_dev->ptr = out_rowptr_.as<int>();
+  C_dev->idx = out_col_.as<int>();
+  C_dev->val = out_val_.as<float>();
+  C_dev->nnz = (int)nnz;
+  C_dev->num_rows = m_;
+  C_dev->num_cols = n_;
+  C_dev->type = ROW_MAJOR;
+  return 0;
+}
+
+int Engine::rowptr64_to_host(long long* host) {
+  if (!have_sym_) return fail(5, "row pointers requested without a successful symbolic pass");
+  SG_CK(cudaMemcpyAsync(host, c_rowptr64_.as<long long>(), sizeof(long long) * ((size_t)m_ + 1),
+                        cudaMemcpyDeviceToHost, stream_),
+        "copy row pointers");
+  SG_CK(cudaStreamSynchronize(stream_), "sync row pointers");
+  return 0;
 }
 
 int Engine::finish_numeric() {
@@ -592,9 +655,9 @@ int Engine::read_status(unsigned* st) {
   return check_status(*st);
 }
 
-int Engine::launch_numeric_bins(int* c_col, float* c_val) {
-  return precision_ == 0 ? launch_numeric_mode<0>(c_col, c_val)
-                         : launch_numeric_mode<1>(c_col, c_val);
+int Engine::launch_numeric_bins(int* c_col, float* c_val, int r0, int r1) {
+  return precision_ == 0 ? launch_numeric_mode<0>(c_col, c_val, r0, r1)
+                         : launch_numeric_mode<1>(c_col, c_val, r0, r1);
 }
 
 size_t Engine::big_dir_bytes() const {
@@ -602,7 +665,7 @@ size_t Engine::big_dir_bytes() const {
 }
 
 template <int MODE>
-int Engine::launch_numeric_mode(int* c_col, float* c_val) {
+int Engine::launch_numeric_mode(int* c_col, float* c_val, int r0, int r1) {
   constexpr int MID_THREADS = 512;
   constexpr size_t VB = sizeof(typename SlotOf<MODE>::T);
   const Operands op = op_;
@@ -613,12 +676,12 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   unsigned* status = &counters_.as<DevCounters>()->status;
   const int stride = 2 * max_row_len_ + 2;
   if (MODE == 0 && rows_cnt_max() > 0)
-    if (int r = launch_num_rows(c_col, c_val)) return r;
+    if (int r = launch_num_rows(c_col, c_val, r0, r1)) return r;
   // big bitmap slices (long rows)
   if (nslices_ > 0) {
     const int dir_words = (int)(big_dir_bytes() / sizeof(uint2));
     const size_t smem = (BIG_THREADS / 32) * SEG_SCRATCH_BYTES + big_dir_bytes() +
-                        (size_t)tn_run_slice_cap_ * ((MODE ? 8 : 4) + sizeof(int));
+                        (size_t)tn_run_slice_cap_ * (MODE ? 8 + sizeof(int) : 4);
     SG_CK(smem_attr(k_num_long<MODE, BIG_THREADS, false>, smem), "smem attr k_num_long");
     const int grid = blocks_for(nslices_, 1, (long long)sms_ * BIG_BLOCKS_PER_SM * 2);
     SG_CK(restrict_scratch_.ensure(sizeof(int) * (size_t)grid * stride), "alloc restrict scratch");
@@ -626,7 +689,8 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     k_num_long<MODE, BIG_THREADS, false><<<grid, BIG_THREADS, smem, stream_>>>(
         op, slices_buf_.as<Slice>(), nslices_, row_p, dir_words, tn_run_slice_cap_,
         restrict_scratch_.as<int>(), stride, bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr);
+        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr,
+        r0, r1);
     SG_LAUNCHED("k_num_long");
   }
   // mid bitmap slices of long rows: at most long_o_num outputs, 512 threads
@@ -643,7 +707,8 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
     k_num_long<MODE, MID_THREADS, true><<<grid, MID_THREADS, smem, stream_>>>(
         op, mid_slices_.as<Slice>(), nmid_, row_p, dir_words, cap,
         restrict_scratch_.as<int>(), 0, bitmaps_.as<unsigned>(), bitmap_words_,
-        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr);
+        long_slot_.as<int>(), c_col, c_val, status, nullptr, nullptr, nullptr, nullptr, nullptr,
+        r0, r1);
     SG_LAUNCHED("k_num_mid");
   }
 #define SG_NUM_BLOCK(L, NT)                                                                  \
@@ -654,7 +719,7 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
       SG_CK(smem_attr(k_num_block<L, NT, MODE>, smem), "smem attr k_num_block");              \
       prof_begin("k_num_block<" #L ">");                                                       \
       k_num_block<L, NT, MODE><<<blocks_for(cnt, 1, (long long)sms_ * 8), NT, smem, stream_>>>( \
-          op, rows + (size_t)b * m, cnt, row_p, c_rowptr, c_col, c_val, status);              \
+          op, rows + (size_t)b * m, cnt, r0, r1, row_p, c_rowptr, c_col, c_val, status);      \
       SG_LAUNCHED("k_num_block");                                                             \
     }                                                                                         \
   }
@@ -663,7 +728,7 @@ int Engine::launch_numeric_mode(int* c_col, float* c_val) {
   return 0;
 }
 
-template int Engine::launch_numeric_mode<0>(int*, float*);
+template int Engine::launch_numeric_mode<0>(int*, float*, int, int);
 
 // Whole-row numeric path: reductions into C (long_rows = 1, any nnz_i) or
 // shared-memory accumulation (long_rows = 2): rows of up to the capacity of
@@ -683,38 +748,53 @@ int Engine::rows_smem_cap(int threads) const {
 
 int Engine::rows_cnt_max() const {
   if (precision_ != 0 || tn_.long_rows == 0 || bitmap_words_ == 0 || n_long_sym_ == 0) return 0;
-  return tn_.long_rows == 1 ? 0x7fffffff : rows_smem_cap(1024);
+  return tn_.long_rows == 2 ? rows_smem_cap(1024) : 0x7fffffff;
 }
 
-int Engine::launch_num_rows(int* c_col, float* c_val) {
+// The whole-row launches of each long_rows mode, as (cnt_min, cnt_max] output
+// ranges: 1 = reductions into C for every row; 2 = shared memory in 512- and
+// 1024-thread blocks (longer rows take column slices); 3 = the same two, and
+// reductions into C above the 1024-thread capacity.
+int Engine::launch_num_rows(int* c_col, float* c_val, int r0, int r1) {
   DevCounters* dc = counters_.as<DevCounters>();
+  if (r0 != 0 || r1 != m_) {  // one of several row ranges: fresh work orders and queues
+    unsigned char* first = reinterpret_cast<unsigned char*>(&dc->lpt_hist);
+    unsigned char* last = reinterpret_cast<unsigned char*>(&dc->row_queue) + sizeof(dc->row_queue);
+    SG_CK(cudaMemsetAsync(first, 0, (size_t)(last - first), stream_), "reset row orders");
+  }
   const int cnt = n_long_sym_;
   const int* rows = sym_rows_.as<int>() + (size_t)FB_LONG * m_;
-  SG_CK(lpt_order_.ensure(sizeof(int) * 2 * (size_t)cnt), "alloc row order");
+  SG_CK(lpt_order_.ensure(sizeof(int) * ROWS_LAUNCHES * (size_t)cnt), "alloc row order");
   const int lb = blocks_for(cnt, 256, (long long)sms_ * 4);
   const Operands op = op_;
   unsigned* status = &dc->status;
-  // (cnt_min, cnt_max] of each launch: one launch for the reduction form,
-  // two block sizes for the shared-memory form
-  const int small_cap = rows_smem_cap(512);
-  const int ranges[2][2] = {{0, tn_.long_rows == 1 ? 0x7fffffff : small_cap},
-                            {small_cap, tn_.long_rows == 1 ? 0 : rows_smem_cap(1024)}};
-  for (int g = 0; g < 2; ++g) {
-    const int cmin = ranges[g][0], cmax = ranges[g][1];
-    if (cmax <= cmin) continue;
+  enum Kind { RED, SMEM512, SMEM1024 };
+  struct Launch { int cmin, cmax; Kind kind; };
+  const int small_cap = rows_smem_cap(512), big_cap = rows_smem_cap(1024);
+  Launch plan[ROWS_LAUNCHES];
+  int nl = 0;
+  if (tn_.long_rows == 1) {
+    plan[nl++] = {0, 0x7fffffff, RED};
+  } else {
+    plan[nl++] = {0, small_cap, SMEM512};
+    plan[nl++] = {small_cap, big_cap, SMEM1024};
+    if (tn_.long_rows == 3) plan[nl++] = {big_cap, 0x7fffffff, RED};
+  }
+  for (int g = 0; g < nl; ++g) {
+    const int cmin = plan[g].cmin, cmax = plan[g].cmax;
     int* order = lpt_order_.as<int>() + (size_t)g * cnt;
     prof_begin("k_lpt_hist");
-    k_lpt_hist<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+    k_lpt_hist<<<lb, 256, 0, stream_>>>(rows, cnt, r0, r1, row_p_.as<long long>(), c_cnt_.as<int>(),
                                         row_span_.as<int2>(), cmin, cmax, ROWS_MAX_WORDS,
                                         dc->lpt_hist[g]);
     SG_LAUNCHED("k_lpt_hist");
     prof_begin("k_lpt_scatter");
-    k_lpt_scatter<<<lb, 256, 0, stream_>>>(rows, cnt, row_p_.as<long long>(), c_cnt_.as<int>(),
+    k_lpt_scatter<<<lb, 256, 0, stream_>>>(rows, cnt, r0, r1, row_p_.as<long long>(), c_cnt_.as<int>(),
                                            row_span_.as<int2>(), cmin, cmax, ROWS_MAX_WORDS,
                                            dc->lpt_hist[g], dc->lpt_cursor[g], order,
                                            &dc->rows_listed[g]);
     SG_LAUNCHED("k_lpt_scatter");
-    if (tn_.long_rows == 1) {
+    if (plan[g].kind == RED) {
       constexpr int NT = ROWS_RED_THREADS;
       const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2);
       SG_CK(smem_attr(k_num_rows<NT, true>, smem), "smem attr k_num_rows");
@@ -724,29 +804,27 @@ int Engine::launch_num_rows(int* c_col, float* c_val) {
           c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
           long_slot_.as<int>(), ROWS_MAX_WORDS, 0, c_col, c_val, status);
       SG_LAUNCHED("k_num_rows");
-    } else if (g == 0) {
+    } else if (plan[g].kind == SMEM512) {
       constexpr int NT = 512;
-      const int cap = small_cap;
       const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
-                          (size_t)cap * sizeof(float);
+                          (size_t)small_cap * sizeof(float);
       SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
       prof_begin("k_num_rows<512>");
       k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_ * 2), NT, smem, stream_>>>(
           op, order, &dc->rows_listed[g], &dc->row_queue[g], row_p_.as<long long>(),
           c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
-          long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
+          long_slot_.as<int>(), ROWS_MAX_WORDS, small_cap, c_col, c_val, status);
       SG_LAUNCHED("k_num_rows");
     } else {
       constexpr int NT = 1024;
-      const int cap = rows_smem_cap(NT);
       const size_t smem = (NT / 32) * SEG_SCRATCH_BYTES + ROWS_MAX_WORDS * sizeof(uint2) +
-                          (size_t)cap * sizeof(float);
+                          (size_t)big_cap * sizeof(float);
       SG_CK(smem_attr(k_num_rows<NT, false>, smem), "smem attr k_num_rows");
       prof_begin("k_num_rows<1024>");
       k_num_rows<NT, false><<<blocks_for(cnt, 1, (long long)sms_), NT, smem, stream_>>>(
           op, order, &dc->rows_listed[g], &dc->row_queue[g], row_p_.as<long long>(),
           c_rowptr64_.as<long long>(), row_span_.as<int2>(), bitmaps_.as<unsigned>(), bitmap_words_,
-          long_slot_.as<int>(), ROWS_MAX_WORDS, cap, c_col, c_val, status);
+          long_slot_.as<int>(), ROWS_MAX_WORDS, big_cap, c_col, c_val, status);
       SG_LAUNCHED("k_num_rows");
     }
   }

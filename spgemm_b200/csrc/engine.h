@@ -35,14 +35,17 @@ struct DevCounters {
   long long grand_total;
   int max_row_len;  // longest row of A (entries)
   int overflow_count;  // warp-bin rows redone by the mid / block kernels
-  // whole-row numeric path, per block size (512 / 1024 threads): rows per
+  // whole-row numeric path, per launch (see launch_num_rows): rows per
   // work group, fill cursors of the work order, rows in the work order and
   // the dynamic row queue
-  int lpt_hist[2][32];
-  int lpt_cursor[2][32];
-  int rows_listed[2];
-  int row_queue[2];
+  int lpt_hist[3][32];
+  int lpt_cursor[3][32];
+  int rows_listed[3];
+  int row_queue[3];
 };
+
+// Whole-row numeric launches per product at most (long_rows = 3).
+constexpr int ROWS_LAUNCHES = 3;
 
 class Engine {
  public:
@@ -72,6 +75,18 @@ class Engine {
   // at their global positions. Allows nnz(C) beyond the int32 range.
   int numeric_batch(int count, const long long* row_off_dev, long long max_rows, int* c_rowptr,
                     int* c_col, float* c_val);
+  // Phase 2 in pieces, for callers that overlap the copy of finished rows
+  // with the rest: numeric_rows() computes C's columns and values of rows
+  // [r0, r1) (stream-ordered, no synchronisation; the ranges of one product
+  // must not overlap and must cover [0, m) before numeric_rowptr), and
+  // numeric_rowptr() writes the int32 row pointers and synchronises once to
+  // check the status word. owned_output() sizes the engine-owned C buffers
+  // for the current symbolic result; rowptr64_to_host() copies C's int64
+  // row pointers (m + 1) to the host and synchronises.
+  int numeric_rows(int* c_col, float* c_val, int r0, int r1);
+  int numeric_rowptr(int* c_rowptr);
+  int owned_output(cm* C_dev);
+  int rowptr64_to_host(long long* host);
   // Both phases into engine-owned output buffers.
   int multiply(const cm& A, const cm& B, cm* C_dev);
   // Numeric pass of the current symbolic result into engine-owned buffers.
@@ -135,15 +150,15 @@ class Engine {
   int finish_numeric();
   int launch_first_pass();
   template <int MODE> int launch_fused();
-  int launch_numeric_bins(int* c_col, float* c_val);
-  template <int MODE> int launch_numeric_mode(int* c_col, float* c_val);
+  int launch_numeric_bins(int* c_col, float* c_val, int r0, int r1);
+  template <int MODE> int launch_numeric_mode(int* c_col, float* c_val, int r0, int r1);
   size_t big_dir_bytes() const;
   // Whole-row numeric path of the long rows (k_num_rows): the largest nnz_i
   // it takes for this product (0: path off), its shared-memory value
   // capacity, and its launch.
   int rows_cnt_max() const;
   int rows_smem_cap(int threads) const;
-  int launch_num_rows(int* c_col, float* c_val);
+  int launch_num_rows(int* c_col, float* c_val, int r0, int r1);
   int scan_counts(const int* in, int n, long long* out);
   int check_status(unsigned st);
   template <class K> cudaError_t smem_attr(K kernel, size_t bytes);

@@ -65,11 +65,17 @@ struct Operands {
 //   8     one block per row, bitmap over the row's column span ("mid")
 // Rows with more products take the two-phase long path:
 //   9     symbolic bitmap count (k_sym_long), numeric later
+// and, for rows the warp bins do not take, ahead of the mid and block bins
+// when the tuning enables it (the default):
+//   10..12 one block of 128 / 256 / 512 threads per row of at most 1024 /
+//         2048 / 4096 products, sorted instead of hashed (k_fused_esc)
 constexpr int FB_WARP_BINS = 5;
 constexpr int FB_BLOCK0 = 5;
 constexpr int FB_MID = 8;
 constexpr int FB_LONG = 9;
-constexpr int FB_COUNT = 10;
+constexpr int FB_ESC0 = 10;
+constexpr int FB_ESC_BINS = 3;
+constexpr int FB_COUNT = 13;
 // Numeric bins of long rows: 4..7 block hash (2^10..2^13 slots), 8 column
 // slices, 9 bitmap of the whole span (statistics slots 0..3 stay unused).
 constexpr int NB_COUNT = 10;
@@ -94,7 +100,11 @@ struct Tuning {
   int mid_cols;         // bitmap paths need a column span of at most this (<= 2^18)
   int long_rows;        // long rows, plain FP32, bitmaps kept: 0 column slices;
                         // 1 whole rows, reductions into C (L2); 2 whole rows,
-                        // shared-memory accumulation (rows up to its capacity)
+                        // shared-memory accumulation (rows up to its capacity;
+                        // longer rows take slices); 3 as 2, reductions into C
+                        // for the longer rows
+  int esc_p_min;        // rows outside the warp bins with esc_p_min < P_i <= long_p
+  int esc_span_min;     // and a span above esc_span_min are sorted (k_fused_esc)
 };
 
 // Whole-row numeric path (k_num_rows): the row's column span must fit the
@@ -129,6 +139,8 @@ __host__ __device__ inline int first_bin_of(long long p, long long cap, int span
     if (lg > lmax) lg = lmax;
     return lg - 6;
   }
+  if (p > t.esc_p_min && span > t.esc_span_min)  // p <= long_p <= 4096
+    return p <= 1024 ? FB_ESC0 : (p <= 2048 ? FB_ESC0 + 1 : FB_ESC0 + 2);
   if (span <= t.mid_cols) return FB_MID;
   int lg = ceil_log2_ll(2 * cap);
   if (lg < 11) lg = 11;

@@ -194,8 +194,9 @@ template <> struct SlotOf<1> { using T = unsigned long long; };  // float2 or do
 // Fused pass, one warp per row: hash accumulate, compact the table in place,
 // sort the occupied entries by column, write the sorted row to the temporary
 // buffer at toff[i] and its length to c_cnt[i]. A row that turns out to have
-// more distinct columns than 4/5 of the table is pushed to the mid list (span
-// within mid_cols) or the largest block list and redone there.
+// more distinct columns than 4/5 of the table is pushed to the sorted bins
+// (when the tuning sorts rows like it), else to the mid list (span within
+// mid_cols) or the largest block list, and redone there.
 //
 // Sorting: tables of 256 slots and more sort packed keys (column offset in
 // the row's span above the slot index; the values stay in their slots) by a
@@ -216,7 +217,8 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
              int* __restrict__ c_cnt, int* __restrict__ t_col, float* __restrict__ t_val,
              int* __restrict__ mid_rows, int* __restrict__ mid_count,
              int* __restrict__ big_rows, int* __restrict__ big_count, int mid_cols,
-             int* __restrict__ overflow_count) {
+             int* __restrict__ esc_rows, int* __restrict__ esc_count, Tuning tn,
+             const long long* __restrict__ row_p, int* __restrict__ overflow_count) {
   constexpr int T = 1 << LOG2T;
   constexpr int LIMIT = T * 4 / 5;
   constexpr int WPB = SW_THREADS / 32;
@@ -243,8 +245,15 @@ k_fused_warp(Operands op, const int* __restrict__ rows, int nrows,
     if (distinct > LIMIT) {  // redo with a larger structure
       if (lane == 0) {
         const int2 sp = row_span[i];
-        if (sp.y + 1 - (sp.x & ~31) <= mid_cols) mid_rows[atomicAdd(mid_count, 1)] = i;
-        else big_rows[atomicAdd(big_count, 1)] = i;
+        const long long p = row_p[i];
+        if (p > tn.esc_p_min && sp.y + 1 - sp.x > tn.esc_span_min && p <= 4096) {
+          const int q = p <= 1024 ? 0 : (p <= 2048 ? 1 : 2);  // sorted bins, as first_bin_of
+          esc_rows[(size_t)q * op.m + atomicAdd(esc_count + q, 1)] = i;
+        } else if (sp.y + 1 - (sp.x & ~31) <= mid_cols) {
+          mid_rows[atomicAdd(mid_count, 1)] = i;
+        } else {
+          big_rows[atomicAdd(big_count, 1)] = i;
+        }
         atomicAdd(overflow_count, 1);
       }
       continue;
@@ -742,21 +751,22 @@ __global__ void k_rowptr_i64_to_i32_shift(const long long* __restrict__ in, int 
 // temporary buffer (slot toff[i], c_cnt[i] entries) to its place in C. One
 // warp per row; rows with tcap == 0 (empty or long) are skipped.
 __global__ void __launch_bounds__(256)
-k_copy_fused(int m, const int* __restrict__ tcap, const long long* __restrict__ toff,
+k_copy_fused(int r0, int r1, const int* __restrict__ tcap, const long long* __restrict__ toff,
              const int* __restrict__ c_cnt, const long long* __restrict__ c_rowptr,
              const int* __restrict__ t_col, const float* __restrict__ t_val,
              int* __restrict__ c_col, float* __restrict__ c_val) {
-  // A warp takes 32 rows at a time: each lane loads one row's length and
-  // offsets (so the 32 rows' loads are in flight together), then the warp
-  // copies the rows one after the other, two entries per lane per step.
+  // Rows [r0, r1). A warp takes 32 rows at a time: each lane loads one row's
+  // length and offsets (so the 32 rows' loads are in flight together), then
+  // the warp copies the rows one after the other, two entries per lane per
+  // step.
   const int lane = threadIdx.x & 31;
   const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long i0 = (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < m;
+  for (long long i0 = r0 + (((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; i0 < r1;
        i0 += warps * 32) {
     const long long i = i0 + lane;
     int n = 0;
     long long src = 0, dst = 0;
-    if (i < m && tcap[i] != 0) {
+    if (i < r1 && tcap[i] != 0) {
       n = c_cnt[i];
       src = toff[i];
       dst = c_rowptr[i];
@@ -881,7 +891,7 @@ k_num_bin(int m, int n, const int* __restrict__ c_cnt, const long long* __restri
 
 template <int LOG2T, int NT, int MODE>
 __global__ void __launch_bounds__(NT)
-k_num_block(Operands op, const int* __restrict__ rows, int nrows,
+k_num_block(Operands op, const int* __restrict__ rows, int nrows, int r0, int r1,
             const long long* __restrict__ row_p, const long long* __restrict__ c_rowptr,
             int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status) {
   constexpr int T = 1 << LOG2T;
@@ -894,6 +904,7 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
   SegScratch* sc = reinterpret_cast<SegScratch*>(smem + T * (sizeof(V) + 4)) + warp;
   for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
     const int i = rows[r];
+    if (i < r0 || i >= r1) continue;  // another row range (block-uniform)
     const long long p = row_p[i];
     for (int t = threadIdx.x; t < T; t += NT) { keys[t] = EMPTY_KEY; vals[t] = V(0); }
     __syncthreads();
@@ -935,12 +946,14 @@ k_num_block(Operands op, const int* __restrict__ rows, int nrows,
 // ---------------------------------------------------------------------------
 
 // Shared memory: per-warp scratch | directory uint2[dir_words] | values[cap]
-// (| sparse mode: l1 bits[dir_words/32 + 1] | touched word list[cap]).
+// | columns[cap] (| sparse mode: l1 bits[dir_words/32 + 1] | touched word
+// list[cap]); plain FP32 slices of long rows have no column array: each
+// slot's column is stored into C by the product that touches it first.
 // The presence bits come from the symbolic pass when it kept them, else from
 // a first expansion pass; a block scan turns popcounts into ranks; the value
 // pass adds every product into the slot given by its column's rank (a
 // counting sort on the column, so the slice comes out in column order); the
-// write-out copies the values in order and expands the bitmap into columns.
+// write-out copies the values (and columns) in order.
 //
 // SPARSE (used for mid rows, at most `cap` outputs over up to 2^18 columns):
 // the directory is cleared once per block and kept clean between slices;
@@ -1011,7 +1024,7 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
            int* __restrict__ c_col, float* __restrict__ c_val, unsigned* status,
            const int* __restrict__ row_list, const int* __restrict__ row_count_p,
            const int2* __restrict__ row_span, const long long* __restrict__ toff,
-           int* __restrict__ c_cnt) {
+           int* __restrict__ c_cnt, int r0, int r1) {
   constexpr int NW = NT / 32;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ long long scan_shm[33];
@@ -1040,6 +1053,7 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       sl = slices[s];
     }
     const int i = sl.row;
+    if (i < r0 || i >= r1) continue;  // another row range's slice (block-uniform)
     const bool fused = (sl.flags & SLICE_FUSED) != 0;
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     int* roff = seg_start + (re - rs);
@@ -1130,6 +1144,12 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
     if (MODE == 1 && pair) {
       LongValTwoSum f{dir, reinterpret_cast<float2*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
       block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
+    } else if (MODE == 0 && !SPARSE) {
+      // each slot's column goes straight to C at its first touch, so the
+      // slice needs shared memory for the values only
+      RowValCols f{dir, reinterpret_cast<float*>(vbase), c_col + sl.out, sl.lo,
+                   (unsigned)(sl.hi - sl.lo)};
+      block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
     } else if (MODE == 0) {
       LongValPlain f{dir, reinterpret_cast<float*>(vbase), cols, sl.lo, (unsigned)(sl.hi - sl.lo)};
       block_walk_row<true>(op, rs, re, whole, seg_start, roff, p, f, sc, warp, NW);
@@ -1150,7 +1170,8 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
       const double* vals = reinterpret_cast<const double*>(vbase);
       block_store_aligned<NT>(c_val + sl.out, ocount, [&](int t) { return finalize_value(vals[t]); });
     }
-    block_store_aligned<NT>(c_col + sl.out, ocount, [&](int t) { return cols[t]; });
+    if (MODE != 0 || SPARSE)
+      block_store_aligned<NT>(c_col + sl.out, ocount, [&](int t) { return cols[t]; });
     if (SPARSE) {
       // leave the directory clean for the next slice
       for (int t = threadIdx.x; t < nt; t += NT) dir[touched[t]] = make_uint2(0u, 0u);
@@ -1167,23 +1188,24 @@ k_num_long(Operands op, const Slice* __restrict__ slices, int nslices,
 // Work order of the long rows: grouped by floor(log2 P_i), heaviest group
 // first, so that on the dynamic row queue of k_num_rows the longest rows
 // start first and the short ones fill in at the end (longest-processing-time
-// first, to a factor of two). Only the rows with more than cnt_min outputs
-// that whole_row_path(cnt_max) accepts are listed.
+// first, to a factor of two). Only the rows of [r0, r1) with more than
+// cnt_min outputs that whole_row_path(cnt_max) accepts are listed.
 constexpr int LPT_GROUPS = 32;
 
 __device__ __forceinline__ int lpt_group(long long p) { return 63 - __clzll(p > 0 ? p : 1); }
 
 __global__ void __launch_bounds__(256)
-k_lpt_hist(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
-           const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_min,
-           int cnt_max, int max_words, int* __restrict__ hist) {
+k_lpt_hist(const int* __restrict__ rows, int nrows, int r0, int r1,
+           const long long* __restrict__ row_p, const int* __restrict__ c_cnt,
+           const int2* __restrict__ row_span, int cnt_min, int cnt_max, int max_words,
+           int* __restrict__ hist) {
   __shared__ int h[LPT_GROUPS];
   if (threadIdx.x < LPT_GROUPS) h[threadIdx.x] = 0;
   __syncthreads();
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
     const int i = rows[r];
     const int o = c_cnt[i];
-    if (o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words))
+    if (i >= r0 && i < r1 && o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words))
       atomicAdd(&h[min(lpt_group(row_p[i]), LPT_GROUPS - 1)], 1);
   }
   __syncthreads();
@@ -1193,10 +1215,11 @@ k_lpt_hist(const int* __restrict__ rows, int nrows, const long long* __restrict_
 // hist: rows per group (from k_lpt_hist); cursor: zeroed per group counters;
 // order: the listed rows, heaviest group first; *nlisted: their count.
 __global__ void __launch_bounds__(256)
-k_lpt_scatter(const int* __restrict__ rows, int nrows, const long long* __restrict__ row_p,
-              const int* __restrict__ c_cnt, const int2* __restrict__ row_span, int cnt_min,
-              int cnt_max, int max_words, const int* __restrict__ hist, int* __restrict__ cursor,
-              int* __restrict__ order, int* __restrict__ nlisted) {
+k_lpt_scatter(const int* __restrict__ rows, int nrows, int r0, int r1,
+              const long long* __restrict__ row_p, const int* __restrict__ c_cnt,
+              const int2* __restrict__ row_span, int cnt_min, int cnt_max, int max_words,
+              const int* __restrict__ hist, int* __restrict__ cursor, int* __restrict__ order,
+              int* __restrict__ nlisted) {
   __shared__ int base[LPT_GROUPS];
   if (threadIdx.x == 0) {
     int run = 0;
@@ -1210,7 +1233,7 @@ k_lpt_scatter(const int* __restrict__ rows, int nrows, const long long* __restri
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nrows; r += gridDim.x * blockDim.x) {
     const int i = rows[r];
     const int o = c_cnt[i];
-    if (o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words)) {
+    if (i >= r0 && i < r1 && o > cnt_min && whole_row_path(o, row_span[i], cnt_max, max_words)) {
       const int g = min(lpt_group(row_p[i]), LPT_GROUPS - 1);
       order[base[g] + atomicAdd(cursor + g, 1)] = i;
     }

@@ -19,7 +19,7 @@ class FakeHandle:
     def __init__(self):
         self.precision = 0
         self.t = {"warp_table_max": 256, "warp_p_max": 4096, "warp_cap_max": 2048,
-                  "long_p": 4096, "mid_cols": 1 << 18, "long_o_num": 4096}
+                  "long_p": 4096, "mid_cols": 1 << 18, "long_o_num": 4096, "esc_p_min": 0}
         self.plans = []
 
     def tuning(self):

@@ -170,7 +170,7 @@ def test_batch_large_warp_tables(precision):
     pairs = small_batch(12, 31, n_lo=3000, n_hi=30000)
     db = DeviceBatch(pairs)
     with sg.Handle(precision) as h:
-        h.set_tuning(warp_table_max=1024, warp_p_max=1024, warp_cap_max=2048)
+        h.set_tuning(warp_table_max=1024, warp_p_max=1024, warp_cap_max=2048, esc_p_min=4096)
         h.batch_plan(db.A, db.B)
         st = h.stats()
         assert st["rows_per_symbolic_bin"][4] > 0  # rows in 1024-slot tables

@@ -21,9 +21,11 @@ def ref_product(A, B, rows=None):
                          rows=rows, stats=True)
 
 
-def check(A, B, precision=sg.PLAIN, a_format="csc", ref=None):
+def check(A, B, precision=sg.PLAIN, a_format="csc", ref=None, tuning=None):
     Aop = A.to_csc() if a_format == "csc" else A
     with sg.Handle(precision) as h:
+        if tuning:
+            h.set_tuning(**tuning)
         C = h.multiply_host(Aop, B)
         stats = h.stats()
     ref = ref_product(A, B) if ref is None else ref
@@ -84,10 +86,14 @@ def test_empty_product():
 
 def test_rmat_all_bins():
     A = W.rmat(14, 16, 1)
-    _, _, stats = check(A, A)
+    _, ref, stats = check(A, A)
     assert stats["rows_per_symbolic_bin"][9] > 0, stats   # long rows
-    assert stats["rows_per_symbolic_bin"][8] > 0, stats   # fused span bitmap
+    assert stats["rows_per_symbolic_bin"][12] > 0, stats  # sorted rows (2K-4K products)
     assert stats["long_row_slices"] == 0, stats           # every long row taken whole
+    # with sorting off, the mid rows take the fused span bitmap
+    _, _, st1 = check(A, A, ref=ref, tuning=dict(esc_p_min=4096))
+    assert st1["rows_per_symbolic_bin"][8] > 0, st1
+    assert sum(st1["rows_per_symbolic_bin"][10:13]) == 0, st1
     # with the whole-row kernel off, long rows take column slices
     with sg.Handle() as h:
         h.set_tuning(long_rows=0)
@@ -176,6 +182,12 @@ TUNINGS = [
     dict(long_rows=2),                                      # whole long rows, shared memory
     dict(long_rows=1, long_p=256, long_o_num=256),          # ... with many short long rows
     dict(long_rows=2, keep_bitmaps=0),                      # no kept bitmaps: column slices
+    dict(long_rows=3),                                      # shared memory, L2 reductions above
+    dict(long_rows=3, long_p=256, long_o_num=256),          # ... with many short long rows
+    dict(warp_cap_max=0),                                   # every fused row sorted
+    dict(esc_p_min=4096),                                   # no sorted rows: bitmap / block hash
+    dict(warp_cap_max=64, esc_p_min=32, esc_span_min=20000),  # sorted only when the span is wide
+    dict(warp_cap_max=0, long_p=1024),                      # sorted rows up to 1024 products
 ]
 
 
@@ -195,7 +207,7 @@ def test_tuning_overrides(tuning, precision):
         assert stats["long_row_slices"] > stats["rows_per_numeric_bin"][8], stats
 
 
-@pytest.mark.parametrize("long_rows", [1, 2])
+@pytest.mark.parametrize("long_rows", [1, 2, 3])
 def test_whole_row_path_with_wide_and_narrow_rows(long_rows):
     """Long rows of both kinds in one product: row 0 has ~90K outputs (beyond
     the shared-memory capacity of long_rows=2, so it takes column slices
@@ -240,7 +252,7 @@ def test_bad_tuning_rejected():
         with pytest.raises(sg.SpgemmError):
             h.set_tuning(warp_table_max=100)
         with pytest.raises(sg.SpgemmError):
-            h.set_tuning(long_rows=3)
+            h.set_tuning(long_rows=4)
 
 
 def _dev(a, dtype, offset=0):
@@ -306,3 +318,98 @@ def test_invalid_inputs_rejected():
         C = h.multiply_host(A.to_csc(), A)
         ref = ref_product(A, A)
         assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+
+
+def _run_twice(A, B, precision, tuning):
+    out = []
+    for _ in range(2):
+        with sg.Handle(precision) as h:
+            h.set_tuning(**tuning)
+            C = h.multiply_host(A, B)  # A as CSR: its entry order is the caller's
+        out.append(C)
+    return out
+
+
+@pytest.mark.parametrize("precision", [sg.PLAIN, sg.COMPENSATED])
+def test_sorted_rows_are_deterministic(precision):
+    # rows merged by sorting sum every column's products in product order
+    # (A's entries in row order, each B row in order), so two runs give the
+    # same bits when A is given as CSR (a CSC A is transposed with atomics,
+    # which leaves the entry order inside a row to arrival order); stencil
+    # rows repeat columns ~6 times each
+    A = W.stencil27(14, seed=3)
+    C1, C2 = _run_twice(A, A, precision, dict(warp_cap_max=0))
+    assert np.array_equal(C1.rowptr, C2.rowptr) and np.array_equal(C1.col, C2.col)
+    assert np.array_equal(C1.val.view(np.uint32), C2.val.view(np.uint32))
+    ref = ref_product(A, A)
+    assert_structure_equal(C1.rowptr, C1.col, ref["rowptr"], ref["col"])
+    tol = plain_tolerance(ref) if precision == sg.PLAIN else compensated_tolerance(ref)
+    assert_values_close(C1.val, ref, tol)
+
+
+def test_sorted_rows_edge_cases():
+    # rows with a single column (one-bit keys), stored zeros and exact
+    # cancellation to an explicit zero, a wide span (25-bit column offsets:
+    # four radix passes), and rows at each sorted-bin capacity (1024 / 2048 /
+    # 4096 products)
+    rng = np.random.default_rng(11)
+    n = 1 << 25
+    # row 0: 64 products all in column 5 (A row of 64 entries, each B row {5})
+    # row 1: products cancelling to zero in column 7; row 2: span ~2^25
+    ra, ca, va, rb, cb, vb = [], [], [], [], [], []
+    for k in range(64):
+        ra.append(0); ca.append(k); va.append(1.0)
+        rb.append(k); cb.append(5); vb.append(float(k % 3) - 1.0)
+    ra += [1, 1]; ca += [64, 65]; va += [2.0, 2.0]
+    rb += [64, 65]; cb += [7, 7]; vb += [1.5, -1.5]
+    for k in range(66, 66 + 300):
+        ra.append(2); ca.append(k); va.append(rng.uniform(-1, 1))
+        rb += [k, k]; cb += [int(rng.integers(0, n // 2)) * 2, n - 1 - 2 * (k - 66)]
+        vb += [rng.uniform(-1, 1), rng.uniform(-1, 1)]
+    A = W.from_coo(3, 400, np.array(ra), np.array(ca), np.array(va, np.float32))
+    B = W.from_coo(400, n, np.array(rb), np.array(cb), np.array(vb, np.float32))
+    C, _, st = check(A, B, tuning=dict(warp_cap_max=0))
+    assert C.col[C.rowptr[1]:C.rowptr[2]].tolist() == [7]
+    assert C.val[C.rowptr[1]:C.rowptr[2]].tolist() == [0.0]  # explicit zero kept
+    assert C.col[0:C.rowptr[1]].tolist() == [5]
+    # full bins: R-MAT rows of up to 4096 products, all sorted
+    A = W.rmat(13, 24, 9)
+    _, _, st = check(A, A, tuning=dict(warp_cap_max=0))
+    assert min(st["rows_per_symbolic_bin"][10:13]) > 0, st
+    check(A, A, sg.COMPENSATED, tuning=dict(warp_cap_max=0))
+
+
+PIECE_TUNINGS = [
+    dict(),                                         # whole long rows (shared memory), sorted mid rows
+    dict(long_rows=0, slice_cap=2048, slice_cols=8192),  # column slices of long rows
+    dict(long_rows=3),                              # whole rows, L2 reductions for the longest
+    dict(long_p=256, long_o_num=256, mid_o_min=0),  # long rows in the span-bitmap and hash bins
+    dict(long_p=256, long_o_num=4096, mid_o_min=100000),  # long rows in the block-hash bins
+]
+
+
+@pytest.mark.parametrize("tuning", PIECE_TUNINGS, ids=lambda t: ",".join(f"{k}={v}" for k, v in t.items()) or "default")
+@pytest.mark.parametrize("precision", [sg.PLAIN, sg.COMPENSATED])
+def test_host_copy_in_pieces(tuning, precision):
+    # the host-buffer calls compute C in row ranges and copy each range back
+    # while the next computes; a 4 KiB piece size gives the maximum of 16
+    # ranges, so every numeric kernel runs on partial row ranges
+    A = W.rmat(13, 16, 2)
+    ref = ref_product(A, A)
+    tol = plain_tolerance(ref) if precision == sg.PLAIN else compensated_tolerance(ref)
+    with sg.Handle(precision) as h:
+        h.set_tuning(**tuning)
+        h.set_copy_chunk(4096)
+        C = h.multiply_host(A.to_csc(), A)
+        assert_structure_equal(C.rowptr, C.col, ref["rowptr"], ref["col"])
+        assert_values_close(C.val, ref, tol)
+        nnz = len(ref["col"])
+        rp = np.full(A.rows + 1, -1, np.int32)
+        col = np.full(nnz, -1, np.int32)
+        val = np.full(nnz, np.nan, np.float32)
+        assert h.multiply_host_to(A.to_csc(), A, rp, col, val) == nnz
+        assert_structure_equal(rp, col, ref["rowptr"], ref["col"])
+        assert_values_close(val, ref, tol)
+        h.set_copy_chunk(0)  # one piece
+        C1 = h.multiply_host(A.to_csc(), A)
+        assert_structure_equal(C1.rowptr, C1.col, ref["rowptr"], ref["col"])
