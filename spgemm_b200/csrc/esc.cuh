@@ -22,7 +22,7 @@
 namespace sg {
 
 constexpr int ESC_KPT = 8;             // products per thread: capacity NT * ESC_KPT
-constexpr int ESC_RADIX_BITS = 8;      // digit bits per radix pass (at most)
+constexpr int ESC_RADIX_BITS = 9;      // digit bits per radix pass (at most)
 constexpr int ESC_BUCKETS = 1 << ESC_RADIX_BITS;
 
 // Partial product as stored for the sort: plain FP32 value, or (rounded
@@ -125,27 +125,12 @@ __device__ __forceinline__ void warp_gather_range(const Operands& op, int rs, in
   }
 }
 
-// Lanes of the warp whose digit equals this lane's: one ballot per digit bit
-// (the lanes agreeing with this lane on every bit).
-__device__ __forceinline__ unsigned digit_peers(unsigned d, int db) {
-  unsigned peers = FULL;
-#pragma unroll
-  for (int b = 0; b < ESC_RADIX_BITS; ++b) {
-    if (b < db) {  // warp-uniform
-      const bool on = (d >> b) & 1u;
-      const unsigned x = __ballot_sync(FULL, on);
-      peers &= on ? x : ~x;
-    }
-  }
-  return peers;
-}
-
 // Stable LSD radix sort of (keys, vals)[0, n) by the low `bits` bits of the
 // key, one block of NT threads, n <= NT * ESC_KPT. Warp w owns groups
 // [w * gpw, (w + 1) * gpw) of 32 consecutive positions (gpw = groups per
 // warp); positions n .. NW * gpw * 32 - 1 must hold EMPTY_KEY (every digit
 // maximal, so they stay behind the row's keys). Per pass: each warp ranks
-// its keys by digit (ballot peers + per-warp counters, in position order),
+// its keys by digit (match.any peers + per-warp counters, in position order),
 // one block scan turns the per-(digit, warp) counts into offsets, and every
 // key is scattered from registers to offset + rank. The sorted sequence ends
 // in buffer 0 or 1 (returned).
@@ -182,7 +167,7 @@ __device__ __forceinline__ int block_radix_sort(unsigned* __restrict__ k0, V* __
         k[g] = sk[p];
         v[g] = sv[p];
         const unsigned d = (k[g] >> sh) & dmask;
-        const unsigned peers = digit_peers(d, db);
+        const unsigned peers = __match_any_sync(FULL, d);
         const int before = wh[d];
         rk[g] = before + __popc(peers & lt);
         __syncwarp();
