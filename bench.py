@@ -260,7 +260,7 @@ class ClockSampler:
 
 # ncu summaries (profiles/) of the dominant kernel's DRAM traffic per launch,
 # by (workload, kernel): the roofline's "traffic" field.
-TRAFFIC_PROFILES = {("rmat18", "k_num_long"): ROOT / "profiles" / "k_num_long_rmat18_traffic.md"}
+TRAFFIC_PROFILES = {("rmat18", "k_num_long"): ROOT / "profiles" / "k_num_long_rmat17_traffic.md"}
 
 
 def profiled_traffic(workload, kernel):
