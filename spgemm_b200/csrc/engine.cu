@@ -116,7 +116,7 @@ Engine::~Engine() {
                    &c_rowptr64_, &tiles_, &sym_rows_, &num_rows_, &long_slot_,
                    &chunk_cnt_, &slices_buf_, &mid_slices_, &row_span_, &counters_, &restrict_scratch_,
                    &tcap_, &toff_, &t_col_, &t_val_,
-                   &bitmaps_, &lpt_order_, &out_rowptr_,
+                   &bitmaps_, &lpt_order_, &valid_starts_, &out_rowptr_,
                    &out_col_, &out_val_};
   for (DevBuf* b : all) b->release();
   for (DevBuf& b : stage_) b.release();
@@ -261,16 +261,34 @@ int Engine::analyze(const cm& A, const cm& B) {
 
   // ---- validate the operands (sync point 1 reports the result) ----
   {
-    const int vb = blocks_for((long long)std::max(kdim_, m) * 32, 256, (long long)sms_ * 16);
+    // flat passes: pointers (marking where B's rows start), then entries
+    const long long grid_cap = (long long)sms_ * 16;
+    const size_t start_words = ((size_t)std::max(B.nnz, 1) + 31) / 32;
+    SG_CK(valid_starts_.ensure(sizeof(unsigned) * start_words), "alloc validation bitmap");
+    unsigned* starts = valid_starts_.as<unsigned>();
+    SG_CK(cudaMemsetAsync(starts, 0, sizeof(unsigned) * start_words, stream_), "memset bitmap");
     prof_begin("k_validate");
-    k_validate<<<vb, 256, 0, stream_>>>(B.ptr, kdim_, B.idx, B.nnz, n_, 1, &dc->status);
-    SG_LAUNCHED("k_validate(B)");
+    k_validate_ptr<<<blocks_for((long long)kdim_ + 1, 256, grid_cap), 256, 0, stream_>>>(
+        B.ptr, kdim_, B.nnz, starts, &dc->status);
+    SG_LAUNCHED("k_validate_ptr(B)");
+    if (B.nnz > 0) {
+      prof_begin("k_validate");
+      k_validate_idx<<<blocks_for(B.nnz, 256, grid_cap), 256, 0, stream_>>>(B.idx, B.nnz, n_, starts,
+                                                                           &dc->status);
+      SG_LAUNCHED("k_validate_idx(B)");
+    }
+    const int a_major = A.type == COL_MAJOR ? kdim_ : m;
+    const int a_minor = A.type == COL_MAJOR ? m : kdim_;
     prof_begin("k_validate");
-    if (A.type == COL_MAJOR)
-      k_validate<<<vb, 256, 0, stream_>>>(A.ptr, kdim_, A.idx, nnz_a, m, 0, &dc->status);
-    else
-      k_validate<<<vb, 256, 0, stream_>>>(A.ptr, m, A.idx, nnz_a, kdim_, 0, &dc->status);
-    SG_LAUNCHED("k_validate(A)");
+    k_validate_ptr<<<blocks_for((long long)a_major + 1, 256, grid_cap), 256, 0, stream_>>>(
+        A.ptr, a_major, nnz_a, nullptr, &dc->status);
+    SG_LAUNCHED("k_validate_ptr(A)");
+    if (nnz_a > 0) {
+      prof_begin("k_validate");
+      k_validate_idx<<<blocks_for(nnz_a, 256, grid_cap), 256, 0, stream_>>>(A.idx, nnz_a, a_minor,
+                                                                           nullptr, &dc->status);
+      SG_LAUNCHED("k_validate_idx(A)");
+    }
     // The transpose and row analysis guard every index they use; their
     // verdict and k_validate's are read at the first synchronisation below,
     // before any kernel trusts the inputs.

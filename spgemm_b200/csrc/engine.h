@@ -196,6 +196,7 @@ class Engine {
   DevBuf sym_rows_, num_rows_, long_slot_, chunk_cnt_, slices_buf_, mid_slices_, row_span_;
   DevBuf tcap_, toff_, t_col_, t_val_;  // fused pass: row bounds, temp offsets, temp output
   DevBuf counters_, restrict_scratch_, bitmaps_, lpt_order_;
+  DevBuf valid_starts_;  // input validation: first position of every row of B (nnz(B) bits)
   int bitmap_words_ = 0;  // per long row; 0 when the bitmaps are not kept
   int max_row_len_ = 0;
   DevBuf out_rowptr_, out_col_, out_val_;

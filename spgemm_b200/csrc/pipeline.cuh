@@ -10,30 +10,32 @@ namespace sg {
 // Input validation
 // ---------------------------------------------------------------------------
 
-// One warp per major index: pointers non-decreasing inside [0, nnz] with
-// ptr[0] == 0 and ptr[n_major] == nnz, minor indices inside [0, n_minor) and,
-// when `sorted` is set, strictly increasing inside each major segment (B's
-// rows must be sorted: the long-row kernels binary-search them). Violations
-// set ST_BAD_INDEX (range) or ST_UNSORTED; nothing is read outside
-// ptr[0..n_major] and idx[0..nnz).
-__global__ void k_validate(const int* __restrict__ ptr, int n_major,
-                           const int* __restrict__ idx, int nnz, int n_minor, int sorted,
-                           unsigned* status) {
-  const int lane = threadIdx.x & 31;
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nw = (gridDim.x * blockDim.x) >> 5;
-  if (gw == 0 && lane == 0 && (ptr[0] != 0 || ptr[n_major] != nnz)) atomicOr(status, ST_BAD_INDEX);
-  for (int i = gw; i < n_major; i += nw) {
-    int s = ptr[i], e = ptr[i + 1];
-    if (s > e || s < 0 || e > nnz) {
-      if (lane == 0) atomicOr(status, ST_BAD_INDEX);
-      continue;
-    }
-    for (int q = s + lane; q < e; q += 32) {
-      const int v = idx[q];
-      if ((unsigned)v >= (unsigned)n_minor) atomicOr(status, ST_BAD_INDEX);
-      if (sorted && q > s && idx[q - 1] >= v) atomicOr(status, ST_UNSORTED);
-    }
+// Input validation as two flat passes (coalesced, one thread per pointer,
+// then one per entry): pointers inside [0, nnz], non-decreasing, ptr[0] == 0
+// and ptr[n_major] == nnz, each segment's first position marked in `starts`
+// (nnz bits, zeroed by the caller; null when sortedness is not checked) ...
+__global__ void k_validate_ptr(const int* __restrict__ ptr, int n_major, int nnz,
+                               unsigned* __restrict__ starts, unsigned* status) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n_major; i += gridDim.x * blockDim.x) {
+    const int s = ptr[i];
+    bool bad = s < 0 || s > nnz || (i == 0 && s != 0) || (i == n_major && s != nnz);
+    if (i < n_major && s > ptr[i + 1]) bad = true;
+    if (bad) atomicOr(status, ST_BAD_INDEX);
+    else if (starts && i < n_major && s < nnz) atomicOr(starts + (s >> 5), 1u << (s & 31));
+  }
+}
+
+// ... then every entry inside [0, n_minor) and, with `starts`, above the
+// entry before it unless it begins a segment (B's rows must be sorted: the
+// long-row kernels binary-search them). Violations set ST_BAD_INDEX (range)
+// or ST_UNSORTED; nothing is read outside ptr[0..n_major] and idx[0..nnz).
+__global__ void k_validate_idx(const int* __restrict__ idx, int nnz, int n_minor,
+                               const unsigned* __restrict__ starts, unsigned* status) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += gridDim.x * blockDim.x) {
+    const int v = idx[q];
+    if ((unsigned)v >= (unsigned)n_minor) atomicOr(status, ST_BAD_INDEX);
+    if (starts && q > 0 && !((starts[q >> 5] >> (q & 31)) & 1u) && idx[q - 1] >= v)
+      atomicOr(status, ST_UNSORTED);
   }
 }
 
