@@ -86,6 +86,7 @@ __global__ void k_transpose_scatter(const int* __restrict__ colptr,
 
 constexpr int RA_THREADS = 256;
 constexpr int RA_ROWS = 64;  // rows per block
+constexpr int RA_UNROLL = 4;  // 32-entry batches of a row in flight together
 
 // Per row i: P_i = sum over A(i,k) of nnz(B(k,:)) (the intermediate product
 // count the reference accumulates per row in initGEMM, src/mm.cu:138-148),
@@ -122,29 +123,49 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     long long acc = 0;
     int lo = 0x7fffffff, hi = -1;  // column span of the row's products
-    for (int b = rs; b < re; b += 32) {
-      const int j = b + lane;
-      long long len = 0;
-      if (j < re) {
-        const int k = op.a_col[j];
-        if ((unsigned)k < (unsigned)op.kdim) {
-          const int bs = op.b_rowptr[k], be = op.b_rowptr[k + 1];
-          if (bs >= 0 && be <= op.nnz_b && bs <= be) {
-            len = be - bs;
-            if (be > bs) {
-              lo = min(lo, op.b_col[bs]);
-              hi = max(hi, op.b_col[be - 1]);
-            }
-          } else {
-            atomicOr(status, ST_BAD_INDEX);
-          }
-        } else {
+    // RA_UNROLL batches of 32 entries at a time, each level of the dependent
+    // loads (A's column, B's row bounds, B's first and last column) issued
+    // for all of them before the next, so a long row of A is not walked one
+    // round trip after another
+    for (int b0 = rs; b0 < re; b0 += 32 * RA_UNROLL) {
+      int k[RA_UNROLL], bs[RA_UNROLL], be[RA_UNROLL];
+      bool ok[RA_UNROLL];
+#pragma unroll
+      for (int u = 0; u < RA_UNROLL; ++u) {
+        const int j = b0 + 32 * u + lane;
+        k[u] = j < re ? op.a_col[j] : 0;
+        ok[u] = j < re;
+        if (ok[u] && (unsigned)k[u] >= (unsigned)op.kdim) {
           atomicOr(status, ST_BAD_INDEX);
+          ok[u] = false;
         }
       }
-      const long long incl = warp_incl_scan64(len);
-      if (j < re) aoff[j] = (int)(acc + incl - len);
-      acc += __shfl_sync(FULL, incl, 31);
+#pragma unroll
+      for (int u = 0; u < RA_UNROLL; ++u) {
+        bs[u] = ok[u] ? op.b_rowptr[k[u]] : 0;
+        be[u] = ok[u] ? op.b_rowptr[k[u] + 1] : 0;
+        if (ok[u] && !(bs[u] >= 0 && be[u] <= op.nnz_b && bs[u] <= be[u])) {
+          atomicOr(status, ST_BAD_INDEX);
+          ok[u] = false;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RA_UNROLL; ++u) {
+        if (ok[u] && be[u] > bs[u]) {
+          lo = min(lo, op.b_col[bs[u]]);
+          hi = max(hi, op.b_col[be[u] - 1]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RA_UNROLL; ++u) {
+        if (b0 + 32 * u < re) {  // warp-uniform
+          const int j = b0 + 32 * u + lane;
+          const long long len = ok[u] ? (long long)(be[u] - bs[u]) : 0;
+          const long long incl = warp_incl_scan64(len);
+          if (j < re) aoff[j] = (int)(acc + incl - len);
+          acc += __shfl_sync(FULL, incl, 31);
+        }
+      }
     }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
