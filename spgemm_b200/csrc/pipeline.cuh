@@ -123,47 +123,78 @@ k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_
     const int rs = op.a_rowptr[i], re = op.a_rowptr[i + 1];
     long long acc = 0;
     int lo = 0x7fffffff, hi = -1;  // column span of the row's products
-    // RA_UNROLL batches of 32 entries at a time, each level of the dependent
-    // loads (A's column, B's row bounds, B's first and last column) issued
-    // for all of them before the next, so a long row of A is not walked one
-    // round trip after another
-    for (int b0 = rs; b0 < re; b0 += 32 * RA_UNROLL) {
-      int k[RA_UNROLL], bs[RA_UNROLL], be[RA_UNROLL];
-      bool ok[RA_UNROLL];
-#pragma unroll
-      for (int u = 0; u < RA_UNROLL; ++u) {
-        const int j = b0 + 32 * u + lane;
-        k[u] = j < re ? op.a_col[j] : 0;
-        ok[u] = j < re;
-        if (ok[u] && (unsigned)k[u] >= (unsigned)op.kdim) {
-          atomicOr(status, ST_BAD_INDEX);
-          ok[u] = false;
-        }
+    // Entry j's B row length and first/last column (invalid indices are
+    // reported and count as empty).
+    auto entry = [&](int j, int& bs, int& be) {
+      const int k = op.a_col[j];
+      bs = be = 0;
+      if ((unsigned)k >= (unsigned)op.kdim) {
+        atomicOr(status, ST_BAD_INDEX);
+        return;
       }
-#pragma unroll
-      for (int u = 0; u < RA_UNROLL; ++u) {
-        bs[u] = ok[u] ? op.b_rowptr[k[u]] : 0;
-        be[u] = ok[u] ? op.b_rowptr[k[u] + 1] : 0;
-        if (ok[u] && !(bs[u] >= 0 && be[u] <= op.nnz_b && bs[u] <= be[u])) {
-          atomicOr(status, ST_BAD_INDEX);
-          ok[u] = false;
-        }
+      const int s0 = op.b_rowptr[k], s1 = op.b_rowptr[k + 1];
+      if (s0 >= 0 && s1 <= op.nnz_b && s0 <= s1) {
+        bs = s0;
+        be = s1;
+      } else {
+        atomicOr(status, ST_BAD_INDEX);
       }
-#pragma unroll
-      for (int u = 0; u < RA_UNROLL; ++u) {
-        if (ok[u] && be[u] > bs[u]) {
-          lo = min(lo, op.b_col[bs[u]]);
-          hi = max(hi, op.b_col[be[u] - 1]);
-        }
+    };
+    if (re - rs <= 32) {  // one batch (most rows)
+      const int j = rs + lane;
+      int bs = 0, be = 0;
+      if (j < re) entry(j, bs, be);
+      if (be > bs) {
+        lo = min(lo, op.b_col[bs]);
+        hi = max(hi, op.b_col[be - 1]);
       }
+      const long long len = be - bs;
+      const long long incl = warp_incl_scan64(len);
+      if (j < re) aoff[j] = (int)(incl - len);
+      acc = __shfl_sync(FULL, incl, 31);
+    } else {
+      // RA_UNROLL batches of 32 entries at a time, each level of the
+      // dependent loads (A's column, B's row bounds, B's first and last
+      // column) issued for all of them before the next, so a long row of A
+      // is not walked one round trip after another
+      for (int b0 = rs; b0 < re; b0 += 32 * RA_UNROLL) {
+        int k[RA_UNROLL], bs[RA_UNROLL], be[RA_UNROLL];
+        bool ok[RA_UNROLL];
 #pragma unroll
-      for (int u = 0; u < RA_UNROLL; ++u) {
-        if (b0 + 32 * u < re) {  // warp-uniform
+        for (int u = 0; u < RA_UNROLL; ++u) {
           const int j = b0 + 32 * u + lane;
-          const long long len = ok[u] ? (long long)(be[u] - bs[u]) : 0;
-          const long long incl = warp_incl_scan64(len);
-          if (j < re) aoff[j] = (int)(acc + incl - len);
-          acc += __shfl_sync(FULL, incl, 31);
+          k[u] = j < re ? op.a_col[j] : 0;
+          ok[u] = j < re;
+          if (ok[u] && (unsigned)k[u] >= (unsigned)op.kdim) {
+            atomicOr(status, ST_BAD_INDEX);
+            ok[u] = false;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < RA_UNROLL; ++u) {
+          bs[u] = ok[u] ? op.b_rowptr[k[u]] : 0;
+          be[u] = ok[u] ? op.b_rowptr[k[u] + 1] : 0;
+          if (ok[u] && !(bs[u] >= 0 && be[u] <= op.nnz_b && bs[u] <= be[u])) {
+            atomicOr(status, ST_BAD_INDEX);
+            ok[u] = false;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < RA_UNROLL; ++u) {
+          if (ok[u] && be[u] > bs[u]) {
+            lo = min(lo, op.b_col[bs[u]]);
+            hi = max(hi, op.b_col[be[u] - 1]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < RA_UNROLL; ++u) {
+          if (b0 + 32 * u < re) {  // warp-uniform
+            const int j = b0 + 32 * u + lane;
+            const long long len = ok[u] ? (long long)(be[u] - bs[u]) : 0;
+            const long long incl = warp_incl_scan64(len);
+            if (j < re) aoff[j] = (int)(acc + incl - len);
+            acc += __shfl_sync(FULL, incl, 31);
+          }
         }
       }
     }
