@@ -205,7 +205,8 @@ int spgemm_batch_copy_all(spgemm_handle_t handle, int* c_rowptr, int* c_colidx,
 
 /* Per-kernel timing: when enabled, CUDA events are recorded on the handle's
  * stream around every engine kernel launch and accumulated per kernel name
- * (collected at the end of each numeric pass). */
+ * (folded when the times are read or reset, which must follow a
+ * synchronisation of the handle's stream, e.g. the end of a numeric pass). */
 int spgemm_set_profiling(spgemm_handle_t handle, int enable);
 int spgemm_reset_kernel_times(spgemm_handle_t handle);
 /* Writes up to max_kernels entries: names ('\n'-separated into `names`),

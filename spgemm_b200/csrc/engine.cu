@@ -95,6 +95,13 @@ void Engine::prof_end() {
   prof_open_.back().b = b;
 }
 
+// Event pairs are folded lazily: when the kernel times are read, or once
+// PROF_DEFER records are open, so that a product's own synchronisation is
+// not followed by host work on every call while profiling is on.
+static constexpr size_t PROF_DEFER = 8192;
+
+int Engine::prof_collect_if_full() { return prof_open_.size() > PROF_DEFER ? prof_collect() : 0; }
+
 int Engine::prof_collect() {
   for (ProfRec& r : prof_open_) {
     if (r.b) {
@@ -463,11 +470,15 @@ int Engine::launch_first_pass() {
     if (tn_.keep_bitmaps && !replay_) {
       const size_t words = (size_t)(n_ + 31) / 32;
       const size_t want = words * 4 * (size_t)cnt;
-      size_t free_b = 0, total_b = 0;
-      cudaMemGetInfo(&free_b, &total_b);
-      const size_t budget = std::min<size_t>((size_t)16 << 30, (free_b + bitmaps_.bytes) / 4);
-      if (want <= budget && bitmaps_.ensure(want) == cudaSuccess) bitmap_words_ = (int)words;
-      cudaGetLastError();  // a failed optional allocation is not an error
+      if (want <= bitmaps_.bytes) {  // the buffer of an earlier product is large enough
+        bitmap_words_ = (int)words;
+      } else {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t budget = std::min<size_t>((size_t)16 << 30, (free_b + bitmaps_.bytes) / 4);
+        if (want <= budget && bitmaps_.ensure(want) == cudaSuccess) bitmap_words_ = (int)words;
+        cudaGetLastError();  // a failed optional allocation is not an error
+      }
     }
     prof_begin("k_sym_long");
     k_sym_long<<<grid, LONG_THREADS, smem, stream_>>>(
@@ -633,7 +644,7 @@ int Engine::finish_numeric() {
                         cudaMemcpyDeviceToHost, stream_),
         "read status");
   SG_CK(cudaStreamSynchronize(stream_), "sync after numeric pass");
-  prof_collect();
+  prof_collect_if_full();
   return check_status(host_counters_->status);
 }
 
@@ -668,7 +679,7 @@ int Engine::read_status(unsigned* st) {
                         cudaMemcpyDeviceToHost, stream_),
         "read status");
   SG_CK(cudaStreamSynchronize(stream_), "sync after batch");
-  prof_collect();
+  prof_collect_if_full();
   *st = host_counters_->status;
   return check_status(*st);
 }

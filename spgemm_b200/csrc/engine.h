@@ -138,9 +138,22 @@ class Engine {
   void prof_begin(const char* name);
   void prof_end();
   int prof_collect();  // after a stream sync: fold finished events into totals
-  void prof_reset() { prof_ms_.clear(); prof_count_.clear(); }
-  const std::map<std::string, double>& prof_ms() const { return prof_ms_; }
-  const std::map<std::string, long long>& prof_count() const { return prof_count_; }
+  int prof_collect_if_full();
+  void prof_reset() {
+    prof_collect();
+    prof_ms_.clear();
+    prof_count_.clear();
+  }
+  // Totals per kernel name (folds the open event pairs first; the stream
+  // must have been synchronised since the last launch).
+  const std::map<std::string, double>& prof_ms() {
+    prof_collect();
+    return prof_ms_;
+  }
+  const std::map<std::string, long long>& prof_count() {
+    prof_collect();
+    return prof_count_;
+  }
 
   int fail(int status, const std::string& msg);
   int cuda_fail(cudaError_t e, const char* what);
