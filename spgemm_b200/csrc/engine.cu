@@ -297,7 +297,7 @@ int Engine::analyze(const cm& A, const cm& B) {
       SG_LAUNCHED("k_validate_idx(A)");
     }
     // The transpose and row analysis guard every index they use; their
-    // verdict and k_validate's are read at the first synchronisation below,
+    // findings and the validation pass's are read at the first synchronisation below,
     // before any kernel trusts the inputs.
   }
 

@@ -95,7 +95,7 @@ constexpr int RA_UNROLL = 4;  // 32-entry batches of a row in flight together
 // span_i) for rows the fused pass computes (0 otherwise), which sizes their
 // slot in the temporary output buffer. Rows are appended to their bin's list
 // with one global atomic per bin per block. B's pointers are range-checked
-// here because k_validate's verdict is only read after this kernel.
+// here because the validation pass's result is only read after this kernel.
 __global__ void __launch_bounds__(RA_THREADS)
 k_row_analysis(Operands op, int* __restrict__ aoff, long long* __restrict__ row_p,
                int* __restrict__ c_cnt, int* __restrict__ tcap, int* __restrict__ fb_count,
